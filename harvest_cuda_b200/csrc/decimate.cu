@@ -1,0 +1,215 @@
+// a2-a3: decimation of every clip to the internal rate and DC removal.
+//
+// WORLD's path (harvest.cpp:43-66, matlabfunctions.cpp:178-204) edge-holds the
+// clip by lag = ceil(140/r)*r samples, reflects 9 more samples at each end
+// (which, because lag > 9, reproduces the held value exactly), runs the order-3
+// low-pass of FilterForDecimate forward and then backward, and keeps every r-th
+// sample. The recurrence is sequential, so it is evaluated here as a blocked
+// state-passing scan:
+//   1. every segment of S samples computes its zero-state final state;
+//   2. one thread per clip chains the segment states with the exact 3x3
+//      transition matrix A^S (precomputed on the host);
+//   3. every segment reruns from its true initial state and writes outputs.
+// Each output therefore follows the reference recurrence sample by sample,
+// differing only by the rounding of the chained initial state.
+#include "hv_stages.cuh"
+
+namespace hv {
+
+
+__device__ __forceinline__ void clip_of_segment(const DecimateView& v, int64_t seg, int& c,
+                                                int64_t& begin, int64_t& end) {
+  c = owner(v.seg_off, v.clips, seg);
+  int64_t k = seg - v.seg_off[c];
+  int64_t total = v.t_off[c + 1] - v.t_off[c];
+  begin = k * v.seg_len;
+  end = begin + v.seg_len < total ? begin + v.seg_len : total;
+}
+
+// Input of the forward pass at padded index i: the held and reflected clip.
+__device__ __forceinline__ double forward_input(const DecimateView& v, const double* x, int c,
+                                                int64_t i) {
+  int64_t n = v.x_off[c + 1] - v.x_off[c];
+  int64_t j = i - 9 - v.lag;
+  j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
+  return x[v.x_off[c] + j];
+}
+
+// One step of FilterForDecimate (matlabfunctions.cpp:118-124); the expression
+// order matches the reference so the step is bit-identical given its state.
+__device__ __forceinline__ double lowpass_step(const DecimateView& v, double in, double& s0,
+                                               double& s1, double& s2) {
+  double w = in + v.a[0] * s0 + v.a[1] * s1 + v.a[2] * s2;
+  double out = v.b[0] * w + v.b[1] * s0 + v.b[1] * s1 + v.b[0] * s2;
+  s2 = s1; s1 = s0; s0 = w;
+  return out;
+}
+
+// Pass 0 reads the padded clip; pass 1 reads the forward output reversed.
+template <int kPass>
+__global__ void decimate_segment_states(DecimateView v, const double* __restrict__ x,
+                                        const double* __restrict__ u, int64_t segments,
+                                        double* __restrict__ states) {
+  int64_t seg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  int c; int64_t begin, end;
+  clip_of_segment(v, seg, c, begin, end);
+  int64_t total = v.t_off[c + 1] - v.t_off[c];
+  const double* uc = u + v.t_off[c];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t i = begin; i < end; ++i) {
+    double in = kPass == 0 ? forward_input(v, x, c, i) : uc[total - 1 - i];
+    lowpass_step(v, in, s0, s1, s2);
+  }
+  states[3 * seg + 0] = s0;
+  states[3 * seg + 1] = s1;
+  states[3 * seg + 2] = s2;
+}
+
+// Chains zero-state segment results into true initial states, in place:
+// on return states[seg] holds the state entering the segment.
+__global__ void decimate_chain(DecimateView v, double* __restrict__ states) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= v.clips) return;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t seg = v.seg_off[c]; seg < v.seg_off[c + 1]; ++seg) {
+    double z0 = states[3 * seg], z1 = states[3 * seg + 1], z2 = states[3 * seg + 2];
+    states[3 * seg] = s0; states[3 * seg + 1] = s1; states[3 * seg + 2] = s2;
+    const double* m = v.trans;
+    double n0 = m[0] * s0 + m[1] * s1 + m[2] * s2 + z0;
+    double n1 = m[3] * s0 + m[4] * s1 + m[5] * s2 + z1;
+    double n2 = m[6] * s0 + m[7] * s1 + m[8] * s2 + z2;
+    s0 = n0; s1 = n1; s2 = n2;
+  }
+}
+
+// Pass 0 writes the forward output u; pass 1 writes the kept samples of the
+// backward output into y (before DC removal).
+template <int kPass>
+__global__ void decimate_segment_run(DecimateView v, const double* __restrict__ x,
+                                     double* __restrict__ u, int64_t segments,
+                                     const double* __restrict__ states, double* __restrict__ y) {
+  int64_t seg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  int c; int64_t begin, end;
+  clip_of_segment(v, seg, c, begin, end);
+  int64_t total = v.t_off[c + 1] - v.t_off[c];
+  double* uc = u + v.t_off[c];
+  double s0 = states[3 * seg], s1 = states[3 * seg + 1], s2 = states[3 * seg + 2];
+  if (kPass == 0) {
+    for (int64_t i = begin; i < end; ++i) uc[i] = lowpass_step(v, forward_input(v, x, c, i), s0, s1, s2);
+    return;
+  }
+  // Kept sample k of the decimated clip sits at backward index
+  // total - 9 - nbeg - (skip + k) * r (matlabfunctions.cpp:195-200).
+  const int r = v.ratio;
+  int64_t m = total - 18;
+  int64_t nout = (m - 1) / r + 1;
+  int64_t nbeg = r - r * nout + m;
+  int64_t skip = v.lag / r;
+  int64_t y_len = v.y_off[c + 1] - v.y_off[c];
+  int64_t anchor = total - 9 - nbeg;  // backward index of decimated sample 0
+  double* yc = y + v.y_off[c];
+  for (int64_t j = begin; j < end; ++j) {
+    double out = lowpass_step(v, uc[total - 1 - j], s0, s1, s2);
+    int64_t dist = anchor - j;
+    if (dist >= 0 && dist % r == 0) {
+      int64_t k = dist / r - skip;
+      if (k >= 0 && k < y_len) yc[k] = out;
+    }
+  }
+}
+
+// Ratio 1: the waveform is used as is (harvest.cpp:45-48).
+__global__ void copy_clips(const double* __restrict__ x, int64_t total, double* __restrict__ y) {
+  int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i < total) y[i] = x[i];
+}
+
+// a3 (harvest.cpp:82-86): y -= mean(y), one block per clip with a fixed
+// reduction tree (deterministic). Also returns the two spectrum bins that
+// WORLD's band filter overwrites (harvest.cpp:116-133): Y[n/2] and Y[n/2-1]
+// of the zero-padded n-point transform, for the final-bin correction.
+__global__ void remove_mean_and_edge_bins(const BatchView v, double* __restrict__ y,
+                                          double* __restrict__ bins /* 3 per clip */) {
+  __shared__ double part[3][32];
+  int c = blockIdx.x;
+  int64_t begin = v.y_off[c], len = v.y_off[c + 1] - begin;
+  double* yc = y + begin;
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) acc += yc[i];
+  // Block reduction of the sum.
+  for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  if (!lane) part[0][warp] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    acc = lane < warps ? part[0][lane] : 0.0;
+    for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (!lane) part[0][0] = acc;
+  }
+  __syncthreads();
+  double mean = part[0][0] / len;
+  __syncthreads();
+  // Subtract, and accumulate Y[n/2] = sum y_j (-1)^j and
+  // Y[n/2-1] = sum y_j (-1)^j e^{+2 pi i j / n}.
+  const int n = v.nfft[c];
+  double ny = 0.0, br = 0.0, bi = 0.0;
+  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
+    double val = yc[i] - mean;
+    yc[i] = val;
+    double sg = (i & 1) ? -val : val;
+    ny += sg;
+    double s, co;
+    sincospi(2.0 * static_cast<double>(i) / n, &s, &co);
+    br += sg * co;
+    bi += sg * s;
+  }
+  for (int o = 16; o; o >>= 1) {
+    ny += __shfl_down_sync(0xffffffffu, ny, o);
+    br += __shfl_down_sync(0xffffffffu, br, o);
+    bi += __shfl_down_sync(0xffffffffu, bi, o);
+  }
+  if (!lane) { part[0][warp] = ny; part[1][warp] = br; part[2][warp] = bi; }
+  __syncthreads();
+  if (warp == 0) {
+    ny = lane < warps ? part[0][lane] : 0.0;
+    br = lane < warps ? part[1][lane] : 0.0;
+    bi = lane < warps ? part[2][lane] : 0.0;
+    for (int o = 16; o; o >>= 1) {
+      ny += __shfl_down_sync(0xffffffffu, ny, o);
+      br += __shfl_down_sync(0xffffffffu, br, o);
+      bi += __shfl_down_sync(0xffffffffu, bi, o);
+    }
+    if (!lane) { bins[3 * c] = ny; bins[3 * c + 1] = br; bins[3 * c + 2] = bi; }
+  }
+}
+
+// Host-side launchers -------------------------------------------------------
+
+cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, double* states,
+                            int64_t segments, double* y, cudaStream_t stream) {
+  const int threads = 128;
+  unsigned grid = static_cast<unsigned>((segments + threads - 1) / threads);
+  unsigned cgrid = static_cast<unsigned>((v.clips + threads - 1) / threads);
+  decimate_segment_states<0><<<grid, threads, 0, stream>>>(v, x, u, segments, states);
+  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
+  decimate_segment_run<0><<<grid, threads, 0, stream>>>(v, x, u, segments, states, y);
+  decimate_segment_states<1><<<grid, threads, 0, stream>>>(v, x, u, segments, states);
+  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
+  decimate_segment_run<1><<<grid, threads, 0, stream>>>(v, x, u, segments, states, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_copy(const double* x, int64_t total, double* y, cudaStream_t stream) {
+  const int threads = 256;
+  copy_clips<<<static_cast<unsigned>((total + threads - 1) / threads), threads, 0, stream>>>(x, total, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_remove_mean(const BatchView& v, double* y, double* bins, cudaStream_t stream) {
+  remove_mean_and_edge_bins<<<v.clips, 1024, 0, stream>>>(v, y, bins);
+  return cudaGetLastError();
+}
+
+}  // namespace hv

@@ -1,0 +1,822 @@
+// Host engine and C ABI of the B200 Harvest engine.
+//
+//   * validation identical to the reference's bindings (src/bindings.cpp:18-39);
+//   * a per-device workspace cache whose clear() never invalidates a call in
+//     flight (src/workspace_cache.h:26-70);
+//   * primary-context handling that restores the caller's context
+//     (src/cuda_device.h:74-108);
+//   * batch planning (parameters of src/engine.cpp:255-266 per clip), one
+//     device arena per workspace, and the launch sequence of the stages,
+//     captured once per batch shape into a CUDA graph and replayed.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <list>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/harvest_b200.h"
+#include "hv_stages.cuh"
+
+namespace hv {
+namespace {
+
+// ---------------------------------------------------------------- errors --
+thread_local std::string g_error;
+
+struct InvalidArgument : std::runtime_error { using std::runtime_error::runtime_error; };
+struct RuntimeFailure : std::runtime_error { using std::runtime_error::runtime_error; };
+
+void check(cudaError_t code, const char* what) {
+  if (code == cudaSuccess) return;
+  const char* name = cudaGetErrorName(code);
+  const char* text = cudaGetErrorString(code);
+  std::string msg = std::string("CUDA: ") + what + ": " + (name ? name : std::to_string(int(code)));
+  if (text) msg += std::string(": ") + text;
+  if (code == cudaErrorMemoryAllocation)
+    msg += ". GPU memory allocation failed; try shorter or fewer clips.";
+  if (code == cudaErrorNoDevice || code == cudaErrorInsufficientDriver)
+    msg += ". Check the NVIDIA driver and CUDA_VISIBLE_DEVICES.";
+  throw RuntimeFailure(msg);
+}
+
+template <class F>
+int guarded(F&& body) {
+  try {
+    body();
+    g_error.clear();
+    return HV_OK;
+  } catch (const InvalidArgument& e) {
+    g_error = e.what();
+    return HV_INVALID_ARGUMENT;
+  } catch (const std::bad_alloc&) {
+    g_error = "host memory allocation failed";
+    return HV_RUNTIME_ERROR;
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return HV_RUNTIME_ERROR;
+  }
+}
+
+// ------------------------------------------------- driver entry points --
+// Resolved through the runtime so the library has no link-time dependency
+// on libcuda (it loads on machines without a GPU driver).
+struct Driver {
+  decltype(&cuInit) init = nullptr;
+  decltype(&cuDevicePrimaryCtxRetain) retain = nullptr;
+  decltype(&cuDevicePrimaryCtxRelease) release = nullptr;
+  decltype(&cuCtxGetCurrent) get_current = nullptr;
+  decltype(&cuCtxSetCurrent) set_current = nullptr;
+  bool ok = false;
+  Driver() {
+    auto get = [](const char* name, void** fn) {
+      cudaDriverEntryPointQueryResult q;
+      return cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) == cudaSuccess && *fn &&
+             q == cudaDriverEntryPointSuccess;
+    };
+    ok = get("cuInit", reinterpret_cast<void**>(&init)) &&
+         get("cuDevicePrimaryCtxRetain", reinterpret_cast<void**>(&retain)) &&
+         get("cuDevicePrimaryCtxRelease", reinterpret_cast<void**>(&release)) &&
+         get("cuCtxGetCurrent", reinterpret_cast<void**>(&get_current)) &&
+         get("cuCtxSetCurrent", reinterpret_cast<void**>(&set_current));
+  }
+};
+const Driver& driver() {
+  static Driver d;
+  return d;
+}
+
+void check_device(int device) {
+  if (device < 0) throw InvalidArgument("device must be a nonnegative visible GPU index");
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    throw RuntimeFailure("CUDA: no usable GPU is visible (" +
+                         std::string(e == cudaSuccess ? "no devices" : cudaGetErrorString(e)) +
+                         "). Check the NVIDIA driver and CUDA_VISIBLE_DEVICES.");
+  }
+  if (device >= count)
+    throw InvalidArgument("device " + std::to_string(device) + " is out of range; " +
+                          std::to_string(count) + " GPU(s) are visible through CUDA_VISIBLE_DEVICES");
+  cudaDeviceProp p{};
+  check(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
+  if (p.major < 10)
+    throw RuntimeFailure("this build targets sm_100a (B200); device " + std::to_string(device) +
+                         " (" + p.name + ") has compute capability " + std::to_string(p.major) +
+                         "." + std::to_string(p.minor));
+}
+
+// Keeps a device's primary context retained while its workspace lives.
+class PrimaryContext {
+ public:
+  explicit PrimaryContext(int device) : device_(device) {
+    const Driver& d = driver();
+    if (!d.ok) throw RuntimeFailure("CUDA driver entry points unavailable");
+    if (d.init(0) != CUDA_SUCCESS) throw RuntimeFailure("cuInit failed");
+    if (d.retain(&ctx_, device) != CUDA_SUCCESS) throw RuntimeFailure("cuDevicePrimaryCtxRetain failed");
+  }
+  ~PrimaryContext() { driver().release(device_); }
+  CUcontext get() const { return ctx_; }
+
+ private:
+  int device_;
+  CUcontext ctx_ = nullptr;
+};
+
+// Makes `target` current and restores the caller's context on exit.
+class ContextGuard {
+ public:
+  explicit ContextGuard(CUcontext target) {
+    const Driver& d = driver();
+    if (d.get_current(&prev_) != CUDA_SUCCESS) throw RuntimeFailure("cuCtxGetCurrent failed");
+    switched_ = prev_ != target;
+    if (switched_ && d.set_current(target) != CUDA_SUCCESS) throw RuntimeFailure("cuCtxSetCurrent failed");
+  }
+  ~ContextGuard() {
+    if (switched_) driver().set_current(prev_);
+  }
+
+ private:
+  CUcontext prev_ = nullptr;
+  bool switched_ = false;
+};
+
+// ------------------------------------------------------------- WORLD maths --
+constexpr double kLog2 = 0.69314718055994529;  // world::kLog2
+
+int matlab_round_host(double v) { return v > 0 ? static_cast<int>(v + 0.5) : static_cast<int>(v - 0.5); }
+int suitable_fft_size(int samples) {  // common.cpp:51-54
+  return static_cast<int>(std::pow(2.0, static_cast<int>(std::log(static_cast<double>(samples)) / kLog2) + 1.0));
+}
+int samples_for(int fs, int64_t n, double period) {  // harvest.cpp:1219-1221
+  return static_cast<int>(1000.0 * n / fs / period) + 1;
+}
+int ratio_for(int fs) { return std::min(12, std::max(1, matlab_round_host(fs / 8000.0))); }
+
+// FilterForDecimate coefficients (matlabfunctions.cpp:27-113), rows by ratio.
+const double kLowA[13][3] = {
+    {0, 0, 0}, {0, 0, 0},
+    {0.041156734567757189, -0.42599112459189636, 0.041037215479961225},
+    {0.95039378983237421, -0.67429146741526791, 0.15412211621346475},
+    {1.4499664446880227, -0.98943497080950582, 0.24578252340690215},
+    {1.7610939654280557, -1.2554914843859768, 0.3237186507788215},
+    {1.9715352749512141, -1.4686795689225347, 0.3893908434965701},
+    {2.1225239019534703, -1.6395144861046302, 0.44469707800587366},
+    {2.2357462340187593, -1.7780899984041358, 0.49152555365968692},
+    {2.3236003491759578, -1.8921545617463598, 0.53148928133729068},
+    {2.3936475118069387, -1.9873904075111861, 0.5658879979027055},
+    {2.450743295230728, -2.06794904601978, 0.59574774438332101},
+    {2.4981398605924205, -2.1368928194784025, 0.62187513816221485}};
+const double kLowB[13][2] = {
+    {0, 0}, {0, 0},
+    {0.16797464681802227, 0.50392394045406674},
+    {0.071221945171178636, 0.21366583551353591},
+    {0.036710750339322612, 0.11013225101796784},
+    {0.021334858522387423, 0.06400457556716227},
+    {0.013469181309343825, 0.040407543928031475},
+    {0.0090366882681608418, 0.027110064804482525},
+    {0.0063522763407111993, 0.019056829022133598},
+    {0.0046331164041389372, 0.013899349212416812},
+    {0.0034818622251927556, 0.010445586675578267},
+    {0.0026822508007163792, 0.0080467524021491377},
+    {0.0021097275904709001, 0.0063291827714127002}};
+
+// validate() of the reference (src/bindings.cpp:18-39), per clip.
+void validate_settings(int64_t n, int fs, double floor, double ceil, double period) {
+  if (n <= 0 || n > INT_MAX) throw InvalidArgument("x must be nonempty and contain at most INT_MAX samples");
+  if (fs < 8000 || fs > 192000) throw InvalidArgument("fs must be between 8000 and 192000 Hz");
+  if (!std::isfinite(floor) || !std::isfinite(ceil) || floor <= 0 || ceil <= floor)
+    throw InvalidArgument("require finite 0 < f0_floor < f0_ceil");
+  int ratio = std::min(12, std::max(1, int(fs / 8000.0 + 0.5)));
+  if (n < int64_t(2) * ratio)
+    throw InvalidArgument("x is too short: require at least two samples after internal decimation");
+  if (ceil >= double(fs) / ratio / 2) throw InvalidArgument("f0_ceil must be below the internal Nyquist frequency");
+  if (!std::isfinite(period) || period <= 0)
+    throw InvalidArgument("frame_period must be finite and positive (milliseconds)");
+  if (1000.0 * n / fs / period >= INT_MAX || 1000.0 * n / fs >= INT_MAX ||
+      double(n) / ratio + 10.0 * fs / ratio / floor >= (1 << 28))
+    throw InvalidArgument("input or analysis settings exceed supported allocation sizes");
+}
+void validate_samples(const double* x, int64_t n) {
+  bool finite = true;
+  for (int64_t i = 0; i < n; ++i) finite &= std::isfinite(x[i]);
+  if (!finite) throw InvalidArgument("x must contain only finite samples");
+}
+
+// ------------------------------------------------------------------- plan --
+struct Settings {
+  int fs;
+  double floor, ceil, period;
+  bool operator<(const Settings& o) const {
+    return std::tie(fs, floor, ceil, period) < std::tie(o.fs, o.floor, o.ceil, o.period);
+  }
+};
+
+// Band-bank tables for one (fs, floor, ceil): centres, half lengths and the
+// reversed, padded taps of GetFilteredSignal (harvest.cpp:101-108) computed
+// with the host's libm exactly as the reference does.
+struct BankTables {
+  int bands = 0, max_pad_taps = 0;
+  std::vector<double> centre;
+  std::vector<int> half;
+  std::vector<int64_t> tap_off;
+  std::vector<double> taps_rev;
+};
+
+BankTables make_bank(int fs, double floor, double ceil) {
+  BankTables t;
+  const int ratio = ratio_for(fs);
+  const double fs_r = double(fs) / ratio;
+  const double lo = floor * 0.9, hi = ceil * 1.1;
+  t.bands = 1 + static_cast<int>(std::log(hi / lo) / kLog2 * 40.0);
+  const int mult = band_bank_tap_multiple();
+  t.tap_off.push_back(0);
+  for (int b = 0; b < t.bands; ++b) {
+    double c = lo * std::pow(2.0, (b + 1) / 40.0);
+    int h = matlab_round_host(fs_r / c * 2.0);
+    int len = 2 * h + 1;
+    std::vector<double> taps(len);
+    for (int i = 0; i < len; ++i) {
+      double tmp = i / (len - 1.0);
+      taps[i] = 0.355768 - 0.487396 * std::cos(2.0 * kPi * tmp) + 0.144232 * std::cos(4.0 * kPi * tmp) -
+                0.012604 * std::cos(6.0 * kPi * tmp);
+    }
+    for (int i = -h; i <= h; ++i) taps[i + h] *= std::cos(2 * kPi * c * i / fs_r);
+    int padded = (len + mult - 1) / mult * mult;
+    for (int j = 0; j < padded; ++j) t.taps_rev.push_back(j < len ? taps[len - 1 - j] : 0.0);
+    t.tap_off.push_back(t.tap_off.back() + padded);
+    t.centre.push_back(c);
+    t.half.push_back(h);
+    t.max_pad_taps = std::max(t.max_pad_taps, padded);
+  }
+  return t;
+}
+
+struct Plan {
+  Settings s;
+  std::vector<int64_t> lengths;
+  int clips = 0, ratio = 1, bands = 0, capacity = 0, per_group = 0, lag = 0;
+  double fs_r = 0;
+  std::shared_ptr<const BankTables> bank;
+  // Host copies of the per-clip tables.
+  std::vector<int64_t> x_off, y_off, t_off, seg_off, frame_off, out_off, scratch_off;
+  std::vector<int> nfft;
+  std::vector<int2> items;
+  int64_t slot_capacity = 0, total_seg = 0;
+  double trans[9];
+  // Device copy of all tables (one allocation) and arena layout.
+  void* meta = nullptr;
+  size_t arena_bytes = 0;
+  struct Layout {
+    size_t x, u, states, y, bins, queue, slots, raw, cand, count, refined, scores, pruned,
+        pruned_scores, best, smoothed, scratch, f0, times;
+  } at{};
+  int bank_ctas = 0;
+  // Device pointers into `meta`.
+  int64_t *d_x_off, *d_y_off, *d_t_off, *d_seg_off, *d_frame_off, *d_out_off, *d_scratch_off, *d_tap_off;
+  int* d_nfft;
+  int* d_half;
+  double *d_centre, *d_taps;
+  int2* d_items;
+  // Captured launch sequence for this plan at a given arena base.
+  cudaGraphExec_t graph = nullptr;
+  void* graph_arena = nullptr;
+  ~Plan() {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (meta) cudaFree(meta);
+  }
+};
+
+constexpr int kSegment = 256;   // decimation scan segment length
+
+void mat3_mul(const double* a, const double* b, double* out) {
+  double r[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) r[3 * i + j] = a[3 * i] * b[j] + a[3 * i + 1] * b[3 + j] + a[3 * i + 2] * b[6 + j];
+  std::memcpy(out, r, sizeof r);
+}
+
+size_t align_up(size_t v) { return (v + 255) / 256 * 256; }
+
+// ------------------------------------------------------------- workspace --
+struct Workspace {
+  int device;
+  PrimaryContext ctx;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t marks[HV_STAGE_COUNT + 1] = {};
+  cudaEvent_t last = nullptr;  // completion of the previous call's work
+  void* arena = nullptr;
+  size_t arena_size = 0;
+  int sms = 0;
+  std::map<Settings, std::shared_ptr<const BankTables>> banks;
+  std::list<std::unique_ptr<Plan>> plans;  // most recent first
+
+  explicit Workspace(int dev) : device(dev), ctx(dev) {
+    ContextGuard g(ctx.get());
+    check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (auto& e : marks) check(cudaEventCreate(&e), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&last, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+  }
+  ~Workspace() {
+    try {
+      ContextGuard g(ctx.get());
+      if (last) cudaEventSynchronize(last);
+      if (stream) cudaStreamSynchronize(stream);
+      plans.clear();
+      if (arena) cudaFree(arena);
+      for (auto& e : marks) if (e) cudaEventDestroy(e);
+      if (last) cudaEventDestroy(last);
+      if (stream) cudaStreamDestroy(stream);
+    } catch (...) {
+    }
+  }
+
+  void ensure_arena(size_t bytes) {
+    if (bytes <= arena_size) return;
+    check(cudaEventSynchronize(last), "cudaEventSynchronize");
+    check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+    if (arena) cudaFree(arena);
+    arena = nullptr;
+    arena_size = 0;
+    for (auto& p : plans) {
+      if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
+    }
+    size_t grow = bytes + bytes / 8;
+    check(cudaMalloc(&arena, grow), "cudaMalloc(workspace)");
+    arena_size = grow;
+  }
+
+  std::shared_ptr<const BankTables> bank_for(const Settings& s) {
+    Settings key{s.fs, s.floor, s.ceil, 0.0};
+    auto it = banks.find(key);
+    if (it != banks.end()) return it->second;
+    auto t = std::make_shared<const BankTables>(make_bank(s.fs, s.floor, s.ceil));
+    if (banks.size() > 8) banks.clear();
+    banks[key] = t;
+    return t;
+  }
+
+  Plan& plan_for(const Settings& s, const int64_t* offsets, int clips) {
+    std::vector<int64_t> lengths(clips);
+    for (int c = 0; c < clips; ++c) lengths[c] = offsets[c + 1] - offsets[c];
+    for (auto it = plans.begin(); it != plans.end(); ++it) {
+      Plan& p = **it;
+      if (p.s.fs == s.fs && p.s.floor == s.floor && p.s.ceil == s.ceil && p.s.period == s.period &&
+          p.lengths == lengths) {
+        plans.splice(plans.begin(), plans, it);
+        return *plans.front();
+      }
+    }
+    auto plan = build_plan(s, std::move(lengths));
+    plans.push_front(std::move(plan));
+    while (plans.size() > 8) plans.pop_back();
+    return *plans.front();
+  }
+
+  std::unique_ptr<Plan> build_plan(const Settings& s, std::vector<int64_t> lengths) {
+    auto p = std::make_unique<Plan>();
+    p->s = s;
+    p->lengths = std::move(lengths);
+    const int B = p->clips = static_cast<int>(p->lengths.size());
+    p->ratio = ratio_for(s.fs);
+    p->fs_r = double(s.fs) / p->ratio;
+    p->bank = bank_for(s);
+    p->bands = p->bank->bands;
+    p->per_group = matlab_round_host(p->bands / 10.0);
+    p->capacity = p->per_group * 7;
+    p->lag = static_cast<int>(std::ceil(140.0 / p->ratio) * p->ratio);
+    const double first = p->bank->centre[0];
+    p->x_off.assign(B + 1, 0); p->y_off.assign(B + 1, 0); p->t_off.assign(B + 1, 0);
+    p->seg_off.assign(B + 1, 0); p->frame_off.assign(B + 1, 0); p->out_off.assign(B + 1, 0);
+    p->scratch_off.assign(B + 1, 0);
+    p->nfft.assign(B, 0);
+    for (int c = 0; c < B; ++c) {
+      int64_t n = p->lengths[c];
+      int y_len = static_cast<int>(std::ceil(double(n) / p->ratio));
+      int64_t total = n + 2 * p->lag + 18;
+      int frames = samples_for(s.fs, n, 1.0);
+      p->x_off[c + 1] = p->x_off[c] + n;
+      p->y_off[c + 1] = p->y_off[c] + y_len;
+      p->t_off[c + 1] = p->t_off[c] + (p->ratio > 1 ? total : 0);
+      p->seg_off[c + 1] = p->seg_off[c] + (p->ratio > 1 ? (total + kSegment - 1) / kSegment : 0);
+      p->frame_off[c + 1] = p->frame_off[c] + frames;
+      p->out_off[c + 1] = p->out_off[c] + samples_for(s.fs, n, s.period);
+      p->scratch_off[c + 1] = p->scratch_off[c] + contour_scratch(frames);
+      p->nfft[c] = suitable_fft_size(y_len + 5 + 2 * static_cast<int>(2.0 * p->fs_r / first));
+      p->slot_capacity = std::max<int64_t>(p->slot_capacity, y_len / 2 + 2);
+    }
+    p->total_seg = p->seg_off[B];
+    // Work items longest first.
+    const BankTables& bank = *p->bank;
+    std::vector<std::pair<int64_t, int2>> items;
+    items.reserve(size_t(B) * p->bands);
+    for (int c = 0; c < B; ++c)
+      for (int b = 0; b < p->bands; ++b) {
+        int64_t y_len = p->y_off[c + 1] - p->y_off[c];
+        int64_t taps = bank.tap_off[b + 1] - bank.tap_off[b];
+        items.push_back({y_len * (taps + 16), make_int2(c, b)});
+      }
+    std::stable_sort(items.begin(), items.end(),
+                     [](const auto& a, const auto& b) { return a.first > b.first; });
+    for (auto& it : items) p->items.push_back(it.second);
+    // A^S for the decimation scan.
+    if (p->ratio > 1) {
+      const double* a = kLowA[p->ratio];
+      double A[9] = {a[0], a[1], a[2], 1, 0, 0, 0, 1, 0};
+      double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+      for (int e = kSegment; e; e >>= 1) {
+        if (e & 1) mat3_mul(R, A, R);
+        mat3_mul(A, A, A);
+      }
+      std::memcpy(p->trans, R, sizeof R);
+    }
+    // Device metadata.
+    std::vector<char> blob;
+    auto put = [&](const void* src, size_t bytes) {
+      size_t at = align_up(blob.size());
+      blob.resize(at + bytes);
+      if (bytes) std::memcpy(blob.data() + at, src, bytes);
+      return at;
+    };
+    size_t o_x = put(p->x_off.data(), 8 * (B + 1)), o_y = put(p->y_off.data(), 8 * (B + 1));
+    size_t o_t = put(p->t_off.data(), 8 * (B + 1)), o_s = put(p->seg_off.data(), 8 * (B + 1));
+    size_t o_f = put(p->frame_off.data(), 8 * (B + 1)), o_o = put(p->out_off.data(), 8 * (B + 1));
+    size_t o_sc = put(p->scratch_off.data(), 8 * (B + 1));
+    size_t o_n = put(p->nfft.data(), 4 * B);
+    size_t o_it = put(p->items.data(), sizeof(int2) * p->items.size());
+    size_t o_c = put(bank.centre.data(), 8 * bank.centre.size());
+    size_t o_h = put(bank.half.data(), 4 * bank.half.size());
+    size_t o_to = put(bank.tap_off.data(), 8 * bank.tap_off.size());
+    size_t o_tp = put(bank.taps_rev.data(), 8 * bank.taps_rev.size());
+    check(cudaMalloc(&p->meta, blob.size()), "cudaMalloc(plan)");
+    check(cudaMemcpy(p->meta, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy(plan)");
+    char* m = static_cast<char*>(p->meta);
+    p->d_x_off = reinterpret_cast<int64_t*>(m + o_x);
+    p->d_y_off = reinterpret_cast<int64_t*>(m + o_y);
+    p->d_t_off = reinterpret_cast<int64_t*>(m + o_t);
+    p->d_seg_off = reinterpret_cast<int64_t*>(m + o_s);
+    p->d_frame_off = reinterpret_cast<int64_t*>(m + o_f);
+    p->d_out_off = reinterpret_cast<int64_t*>(m + o_o);
+    p->d_scratch_off = reinterpret_cast<int64_t*>(m + o_sc);
+    p->d_nfft = reinterpret_cast<int*>(m + o_n);
+    p->d_items = reinterpret_cast<int2*>(m + o_it);
+    p->d_centre = reinterpret_cast<double*>(m + o_c);
+    p->d_half = reinterpret_cast<int*>(m + o_h);
+    p->d_tap_off = reinterpret_cast<int64_t*>(m + o_to);
+    p->d_taps = reinterpret_cast<double*>(m + o_tp);
+    // Arena layout.
+    int per_sm = band_bank_ctas_per_sm(bank.max_pad_taps);
+    if (per_sm < 1) throw RuntimeFailure("band-bank kernel does not fit on this device");
+    int items_n = static_cast<int>(p->items.size());
+    p->bank_ctas = std::max(1, std::min(items_n, sms * per_sm));
+    const int64_t F = p->frame_off[B];
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t at = off; off = align_up(off + bytes); return at; };
+    p->at.x = take(8 * p->x_off[B]);
+    p->at.u = take(8 * p->t_off[B]);
+    p->at.states = take(8 * 3 * p->total_seg);
+    p->at.y = take(8 * p->y_off[B]);
+    p->at.bins = take(8 * 3 * B);
+    p->at.queue = take(16);
+    p->at.slots = take(8 * 4 * p->slot_capacity * p->bank_ctas);
+    p->at.raw = take(8 * size_t(p->bands) * F);
+    p->at.cand = take(8 * size_t(p->per_group) * F);
+    p->at.count = take(4 * B);
+    p->at.refined = take(8 * size_t(p->capacity) * F);
+    p->at.scores = take(8 * size_t(p->capacity) * F);
+    p->at.pruned = take(8 * size_t(p->capacity) * F);
+    p->at.pruned_scores = take(8 * size_t(p->capacity) * F);
+    p->at.best = take(8 * F);
+    p->at.smoothed = take(8 * F);
+    p->at.scratch = take(8 * p->scratch_off[B]);
+    p->at.f0 = take(8 * p->out_off[B]);
+    p->at.times = take(8 * p->out_off[B]);
+    p->arena_bytes = off;
+    return p;
+  }
+
+  template <class T>
+  T* ptr(size_t at) const { return reinterpret_cast<T*>(static_cast<char*>(arena) + at); }
+
+  // Enqueues every stage on `s`. With `marks_on`, records stage events.
+  void enqueue(Plan& p, cudaStream_t s, bool marks_on) {
+    const int B = p.clips;
+    const int64_t F = p.frame_off[B];
+    BatchView bv{};
+    bv.clips = B; bv.ratio = p.ratio; bv.bands = p.bands; bv.capacity = p.capacity;
+    bv.per_group = p.per_group; bv.fs_r = p.fs_r; bv.f0_floor = p.s.floor; bv.f0_ceil = p.s.ceil;
+    bv.x_off = p.d_x_off; bv.y_off = p.d_y_off; bv.frame_off = p.d_frame_off; bv.nfft = p.d_nfft;
+    auto mark = [&](int i) { if (marks_on) check(cudaEventRecord(marks[i], s), "cudaEventRecord"); };
+    double* x = ptr<double>(p.at.x);
+    double* y = ptr<double>(p.at.y);
+    mark(0);
+    if (p.ratio > 1) {
+      DecimateView dv{};
+      dv.clips = B; dv.ratio = p.ratio; dv.lag = p.lag; dv.seg_len = kSegment;
+      std::memcpy(dv.a, kLowA[p.ratio], sizeof dv.a);
+      std::memcpy(dv.b, kLowB[p.ratio], sizeof dv.b);
+      std::memcpy(dv.trans, p.trans, sizeof dv.trans);
+      dv.x_off = p.d_x_off; dv.y_off = p.d_y_off; dv.t_off = p.d_t_off; dv.seg_off = p.d_seg_off;
+      check(launch_decimate(dv, x, ptr<double>(p.at.u), ptr<double>(p.at.states), p.total_seg, y, s),
+            "decimate");
+    } else {
+      check(launch_copy(x, p.x_off[B], y, s), "copy");
+    }
+    check(launch_remove_mean(bv, y, ptr<double>(p.at.bins), s), "remove_mean");
+    mark(1);
+    BankView kv{};
+    kv.batch = bv;
+    kv.centre = p.d_centre; kv.half = p.d_half; kv.tap_off = p.d_tap_off; kv.taps_rev = p.d_taps;
+    kv.items = p.d_items; kv.item_count = static_cast<int>(p.items.size());
+    kv.max_pad_taps = p.bank->max_pad_taps; kv.total_frames = F; kv.slot_capacity = p.slot_capacity;
+    check(cudaMemsetAsync(ptr<int>(p.at.queue), 0, 16, s), "memset");
+    check(launch_band_bank(kv, y, ptr<double>(p.at.bins), ptr<int>(p.at.queue), ptr<double>(p.at.slots),
+                           p.bank_ctas, ptr<double>(p.at.raw), s),
+          "band_bank");
+    mark(2);
+    check(cudaMemsetAsync(ptr<int>(p.at.count), 0, 4 * B, s), "memset");
+    check(launch_candidates(bv, ptr<double>(p.at.raw), F, ptr<double>(p.at.cand), ptr<int>(p.at.count), s),
+          "candidates");
+    mark(3);
+    check(launch_refine(bv, y, ptr<double>(p.at.cand), ptr<int>(p.at.count), F, ptr<double>(p.at.refined),
+                        ptr<double>(p.at.scores), s),
+          "refine");
+    mark(4);
+    check(launch_prune(bv, ptr<double>(p.at.refined), ptr<double>(p.at.scores), ptr<int>(p.at.count), F,
+                       ptr<double>(p.at.pruned), ptr<double>(p.at.pruned_scores), ptr<double>(p.at.best), s),
+          "prune");
+    mark(5);
+    ContourView cv{};
+    cv.batch = bv;
+    cv.pruned = ptr<double>(p.at.pruned); cv.pruned_scores = ptr<double>(p.at.pruned_scores);
+    cv.best = ptr<double>(p.at.best); cv.count = ptr<int>(p.at.count);
+    cv.scratch_off = p.d_scratch_off; cv.scratch = ptr<double>(p.at.scratch);
+    cv.smoothed = ptr<double>(p.at.smoothed); cv.period = p.s.period; cv.out_off = p.d_out_off;
+    cv.f0_out = ptr<double>(p.at.f0); cv.t_out = ptr<double>(p.at.times);
+    check(launch_contour(cv, s), "contour");
+    mark(6);
+  }
+
+  // Runs the compute of `p` on stream `s`, through the plan's graph when
+  // allowed. Inputs are in the arena's x region; outputs land in f0/times.
+  void run(Plan& p, cudaStream_t s, bool use_graph, bool marks_on) {
+    if (!use_graph || marks_on) {
+      enqueue(p, s, marks_on);
+      return;
+    }
+    if (!p.graph || p.graph_arena != arena) {
+      if (p.graph) { cudaGraphExecDestroy(p.graph); p.graph = nullptr; }
+      cudaGraph_t g = nullptr;
+      check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+      try {
+        enqueue(p, stream, false);
+      } catch (...) {
+        cudaStreamEndCapture(stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+      }
+      check(cudaStreamEndCapture(stream, &g), "cudaStreamEndCapture");
+      cudaError_t e = cudaGraphInstantiate(&p.graph, g, 0);
+      cudaGraphDestroy(g);
+      check(e, "cudaGraphInstantiate");
+      p.graph_arena = arena;
+    }
+    check(cudaGraphLaunch(p.graph, s), "cudaGraphLaunch");
+  }
+};
+
+// One workspace per device behind a lease; clear() retires them without
+// invalidating leases in flight (same contract as the reference's cache).
+class WorkspaceCache {
+  struct Slot {
+    std::mutex mutex;
+    std::unique_ptr<Workspace> ws;
+  };
+  std::mutex mutex_;
+  std::map<int, std::shared_ptr<Slot>> slots_;
+  uint64_t generation_ = 0;
+
+ public:
+  class Lease {
+    std::shared_ptr<Slot> slot_;
+    std::unique_lock<std::mutex> lock_;
+
+   public:
+    Lease(WorkspaceCache& cache, int device) {
+      uint64_t gen;
+      {
+        std::lock_guard<std::mutex> l(cache.mutex_);
+        gen = cache.generation_;
+        auto it = cache.slots_.find(device);
+        if (it != cache.slots_.end()) slot_ = it->second;
+      }
+      if (!slot_) {
+        auto created = std::make_shared<Slot>();
+        created->ws = std::make_unique<Workspace>(device);
+        std::lock_guard<std::mutex> l(cache.mutex_);
+        slot_ = gen == cache.generation_ ? cache.slots_.try_emplace(device, created).first->second : created;
+      }
+      lock_ = std::unique_lock<std::mutex>(slot_->mutex);
+    }
+    Workspace& get() const { return *slot_->ws; }
+  };
+  void clear() {
+    std::map<int, std::shared_ptr<Slot>> retired;
+    {
+      std::lock_guard<std::mutex> l(mutex_);
+      ++generation_;
+      retired.swap(slots_);
+    }
+  }
+};
+
+WorkspaceCache& cache() {
+  static WorkspaceCache* c = new WorkspaceCache();  // outlives static teardown order
+  return *c;
+}
+
+const char* kStageNames[HV_STAGE_COUNT] = {"decimate", "band_bank", "candidates", "refine", "prune", "contour"};
+
+// Shared body of the host-pointer entry points.
+void run_host(const double* x, const int64_t* offsets, int clips, const Settings& s, int device,
+              double* f0, double* times, bool use_graph, double* stage_ms) {
+  check_device(device);
+  WorkspaceCache::Lease lease(cache(), device);
+  Workspace& ws = lease.get();
+  ContextGuard guard(ws.ctx.get());
+  Plan& p = ws.plan_for(s, offsets, clips);
+  ws.ensure_arena(p.arena_bytes);
+  const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
+  check(cudaStreamWaitEvent(ws.stream, ws.last, 0), "cudaStreamWaitEvent");
+  check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyHostToDevice, ws.stream),
+        "cudaMemcpy(x)");
+  ws.run(p, ws.stream, use_graph, stage_ms != nullptr);
+  check(cudaMemcpyAsync(f0, ws.ptr<double>(p.at.f0), 8 * total_out, cudaMemcpyDeviceToHost, ws.stream),
+        "cudaMemcpy(f0)");
+  if (times)
+    check(cudaMemcpyAsync(times, ws.ptr<double>(p.at.times), 8 * total_out, cudaMemcpyDeviceToHost, ws.stream),
+          "cudaMemcpy(times)");
+  check(cudaEventRecord(ws.last, ws.stream), "cudaEventRecord");
+  check(cudaStreamSynchronize(ws.stream), "harvest");
+  if (stage_ms)
+    for (int i = 0; i < HV_STAGE_COUNT; ++i) {
+      float ms = 0;
+      check(cudaEventElapsedTime(&ms, ws.marks[i], ws.marks[i + 1]), "cudaEventElapsedTime");
+      stage_ms[i] = ms;
+    }
+}
+
+}  // namespace
+}  // namespace hv
+
+using namespace hv;
+
+extern "C" {
+
+const char* hv_last_error(void) { return g_error.c_str(); }
+
+int hv_cuda_available(int device) {
+  if (device < 0) return 0;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) { cudaGetLastError(); return 0; }
+  if (device >= count) return 0;
+  cudaDeviceProp p{};
+  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) { cudaGetLastError(); return 0; }
+  return p.major >= 10 ? 1 : 0;
+}
+
+int64_t hv_output_length(int64_t n, int fs, double frame_period) {
+  if (n <= 0 || fs <= 0 || !(frame_period > 0) || !std::isfinite(frame_period)) return -1;
+  double v = 1000.0 * n / fs / frame_period;
+  if (!(v < INT_MAX)) return -1;
+  return samples_for(fs, n, frame_period);
+}
+
+int hv_validate(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil, double frame_period) {
+  return guarded([&] {
+    validate_settings(n, fs, f0_floor, f0_ceil, frame_period);
+    if (!x) throw InvalidArgument("x is null");
+    validate_samples(x, n);
+  });
+}
+
+int hv_harvest(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil, double frame_period,
+               int device, double* f0, double* times, int64_t out_len) {
+  return guarded([&] {
+    validate_settings(n, fs, f0_floor, f0_ceil, frame_period);
+    if (!x || !f0 || !times) throw InvalidArgument("null buffer");
+    validate_samples(x, n);
+    if (out_len != samples_for(fs, n, frame_period)) throw InvalidArgument("output length mismatch");
+    int64_t offsets[2] = {0, n};
+    run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, nullptr);
+  });
+}
+
+int hv_profile(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil, double frame_period,
+               int device, double* f0, double* times, int64_t out_len, double* stage_ms) {
+  return guarded([&] {
+    validate_settings(n, fs, f0_floor, f0_ceil, frame_period);
+    if (!x || !f0 || !times || !stage_ms) throw InvalidArgument("null buffer");
+    validate_samples(x, n);
+    if (out_len != samples_for(fs, n, frame_period)) throw InvalidArgument("output length mismatch");
+    int64_t offsets[2] = {0, n};
+    run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, stage_ms);
+  });
+}
+
+const char* hv_stage_name(int stage) {
+  return stage >= 0 && stage < HV_STAGE_COUNT ? kStageNames[stage] : "";
+}
+
+int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs, double f0_floor,
+                     double f0_ceil, double frame_period, int device, double* f0, double* times,
+                     unsigned flags, void* stream) {
+  return guarded([&] {
+    if (clips <= 0 || !offsets) throw InvalidArgument("a batch needs at least one clip and its offsets");
+    if (!x || !f0) throw InvalidArgument("null buffer");
+    for (int c = 0; c < clips; ++c) {
+      if (offsets[c + 1] < offsets[c]) throw InvalidArgument("offsets must be nondecreasing");
+      validate_settings(offsets[c + 1] - offsets[c], fs, f0_floor, f0_ceil, frame_period);
+    }
+    Settings s{fs, f0_floor, f0_ceil, frame_period};
+    const bool use_graph = !(flags & HV_NO_GRAPH);
+    if (!(flags & HV_DEVICE_POINTERS)) {
+      validate_samples(x + offsets[0], offsets[clips] - offsets[0]);
+      run_host(x, offsets, clips, s, device, f0, times, use_graph, nullptr);
+      return;
+    }
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ws.stream;
+    Plan& p = ws.plan_for(s, offsets, clips);
+    ws.ensure_arena(p.arena_bytes);
+    const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
+    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
+    check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyDeviceToDevice, st),
+          "cudaMemcpy(x)");
+    ws.run(p, st, use_graph, false);
+    check(cudaMemcpyAsync(f0, ws.ptr<double>(p.at.f0), 8 * total_out, cudaMemcpyDeviceToDevice, st),
+          "cudaMemcpy(f0)");
+    if (times)
+      check(cudaMemcpyAsync(times, ws.ptr<double>(p.at.times), 8 * total_out, cudaMemcpyDeviceToDevice, st),
+            "cudaMemcpy(times)");
+    // The workspace is reused by the next call on this device, on whatever
+    // stream; that call waits for this event first.
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
+  });
+}
+
+int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil, int device,
+                      double* y, double* raw, int* count, double* cand, double* refined, double* scores,
+                      double* pruned, double* pruned_scores, double* best, double* smoothed) {
+  return guarded([&] {
+    validate_settings(n, fs, f0_floor, f0_ceil, 5.0);
+    if (!x) throw InvalidArgument("null buffer");
+    validate_samples(x, n);
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    int64_t offsets[2] = {0, n};
+    Plan& p = ws.plan_for(Settings{fs, f0_floor, f0_ceil, 5.0}, offsets, 1);
+    ws.ensure_arena(p.arena_bytes);
+    check(cudaStreamWaitEvent(ws.stream, ws.last, 0), "cudaStreamWaitEvent");
+    check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x, 8 * n, cudaMemcpyHostToDevice, ws.stream), "cudaMemcpy(x)");
+    ws.run(p, ws.stream, false, false);
+    const int64_t F = p.frame_off[1];
+    auto out = [&](void* dst, size_t at, size_t bytes) {
+      if (dst) check(cudaMemcpyAsync(dst, ws.ptr<char>(at), bytes, cudaMemcpyDeviceToHost, ws.stream), "cudaMemcpy");
+    };
+    out(y, p.at.y, 8 * p.y_off[1]);
+    out(raw, p.at.raw, 8 * size_t(p.bands) * F);
+    out(count, p.at.count, 4);
+    out(cand, p.at.cand, 8 * size_t(p.per_group) * F);
+    out(refined, p.at.refined, 8 * size_t(p.capacity) * F);
+    out(scores, p.at.scores, 8 * size_t(p.capacity) * F);
+    out(pruned, p.at.pruned, 8 * size_t(p.capacity) * F);
+    out(pruned_scores, p.at.pruned_scores, 8 * size_t(p.capacity) * F);
+    out(best, p.at.best, 8 * F);
+    out(smoothed, p.at.smoothed, 8 * F);
+    check(cudaEventRecord(ws.last, ws.stream), "cudaEventRecord");
+    check(cudaStreamSynchronize(ws.stream), "harvest_stages");
+  });
+}
+
+int hv_clear_cache(void) {
+  return guarded([&] { cache().clear(); });
+}
+
+}  // extern "C"

@@ -1,0 +1,74 @@
+// Stage interfaces: the views each kernel family receives and the host-side
+// launchers the engine calls. Included by the kernels and by engine.cu.
+#pragma once
+#include "hv_device.cuh"
+
+namespace hv {
+
+struct DecimateView {
+  int clips;
+  int ratio;
+  int lag;
+  int seg_len;                 // S
+  double a[3], b[2];           // FilterForDecimate coefficients for `ratio`
+  double trans[9];             // A^S, row-major
+  const int64_t* x_off;        // [clips + 1]
+  const int64_t* y_off;        // [clips + 1]
+  const int64_t* t_off;        // [clips + 1] padded-sequence offsets (T_c = n + 2 lag + 18)
+  const int64_t* seg_off;      // [clips + 1] segment offsets
+};
+
+struct BankView {
+  BatchView batch;
+  const double* centre;      // [bands] band centre frequency
+  const int* half;           // [bands] filter half length
+  const int64_t* tap_off;    // [bands + 1] reversed taps, padded to kFirR
+  const double* taps_rev;    // reversed taps, zero padded
+  const int2* items;         // (clip, band), longest first
+  int item_count;
+  int max_pad_taps;          // max padded tap count over bands
+  int64_t total_frames;
+  int64_t slot_capacity;     // events per kind per CTA slot
+};
+
+struct ContourView {
+  BatchView batch;
+  const double* pruned;         // [frames][capacity]
+  const double* pruned_scores;  // [frames][capacity]
+  const double* best;           // [frames] SearchF0Base
+  const int* count;             // [clips]
+  const int64_t* scratch_off;   // [clips + 1] in doubles
+  double* scratch;
+  double* smoothed;             // [frames] 1 ms contour
+  double period;                // frame_period in ms
+  const int64_t* out_off;       // [clips + 1]
+  double* f0_out;
+  double* t_out;
+};
+
+cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, double* states,
+                            int64_t segments, double* y, cudaStream_t stream);
+cudaError_t launch_copy(const double* x, int64_t total, double* y, cudaStream_t stream);
+cudaError_t launch_remove_mean(const BatchView& v, double* y, double* bins, cudaStream_t stream);
+
+size_t band_bank_smem_bytes(int max_pad_taps);
+int band_bank_tap_multiple();
+int band_bank_threads();
+int band_bank_ctas_per_sm(int max_pad_taps);
+cudaError_t launch_band_bank(const BankView& v, const double* y, const double* edge_bins,
+                             int* queue, double* slots, int ctas, double* raw,
+                             cudaStream_t stream);
+
+cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t total_frames,
+                              double* cand, int* count, cudaStream_t stream);
+cudaError_t launch_refine(const BatchView& v, const double* y, const double* cand,
+                          const int* count, int64_t total_frames, double* refined,
+                          double* scores, cudaStream_t stream);
+cudaError_t launch_prune(const BatchView& v, const double* refined, const double* scores,
+                         const int* count, int64_t total_frames, double* pruned,
+                         double* pruned_scores, double* best, cudaStream_t stream);
+
+int64_t contour_scratch(int64_t frames);
+cudaError_t launch_contour(const ContourView& v, cudaStream_t stream);
+
+}  // namespace hv

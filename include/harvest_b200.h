@@ -1,0 +1,106 @@
+/*
+ * harvest_b200.h — C ABI of the B200 Harvest F0 engine (libharvest_b200.so).
+ *
+ * Plain pointers and sizes only; no exceptions cross this boundary. Every
+ * entry point returns a status code; on failure a message for the calling
+ * thread is available from hv_last_error(). The Python package maps
+ * HV_INVALID_ARGUMENT to ValueError and HV_RUNTIME_ERROR to RuntimeError,
+ * which is how the reference's nanobind layer reports the same failures
+ * (reference src/bindings.cpp:18-39, src/cuda_device.h:8-40).
+ *
+ * Threading: calls may come from any thread. Calls on one device take turns
+ * on that device's cached workspace; calls on different devices run in
+ * parallel (reference src/workspace_cache.h:10-12). The caller's current
+ * CUDA context is restored before every call returns (reference
+ * src/cuda_device.h:90-108).
+ */
+#ifndef HARVEST_B200_H_
+#define HARVEST_B200_H_
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HV_API __attribute__((visibility("default")))
+#else
+#define HV_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HV_OK 0
+#define HV_INVALID_ARGUMENT 1 /* bad sizes, rates, ranges, samples or device index */
+#define HV_RUNTIME_ERROR 2    /* no usable GPU, CUDA failure, out of memory */
+
+/* Flags for hv_harvest_batch. */
+#define HV_DEVICE_POINTERS 1u /* x, f0 and times are device pointers on `device` */
+#define HV_NO_GRAPH 2u        /* launch stage by stage instead of replaying a CUDA graph */
+
+/* Message describing the last failure on the calling thread ("" if none). */
+HV_API const char* hv_last_error(void);
+
+/* 1 if `device` is a visible GPU this library can run on, else 0. Never
+ * fails (reference bindings.cpp:66-67, cuda_available). */
+HV_API int hv_cuda_available(int device);
+
+/* Number of output frames for n samples at fs and frame_period (ms), as
+ * GetSamplesForHarvest (reference third_party/world/src/harvest.cpp:1219);
+ * -1 if the arguments are invalid. */
+HV_API int64_t hv_output_length(int64_t n, int fs, double frame_period);
+
+/* Checks one clip's arguments and samples exactly as the reference's
+ * validate() (reference src/bindings.cpp:18-39). */
+HV_API int hv_validate(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil,
+                double frame_period);
+
+/* Harvest on one clip of host memory; replaces the reference's
+ * _core.harvest (reference src/bindings.cpp:68-80) and analyze()
+ * (reference src/engine.cpp:240-333). f0 and times receive
+ * hv_output_length(n, fs, frame_period) values (out_len must equal it). */
+HV_API int hv_harvest(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil,
+               double frame_period, int device, double* f0, double* times, int64_t out_len);
+
+/* Harvest on `clips` clips packed back to back: clip c is
+ * x[offsets[c] .. offsets[c+1]). offsets (clips + 1 entries) is host memory.
+ * Outputs are packed the same way with per-clip lengths
+ * hv_output_length(offsets[c+1] - offsets[c], fs, frame_period). With
+ * HV_DEVICE_POINTERS, x/f0/times are device memory and the work is ordered
+ * on `stream` (a cudaStream_t, NULL for the engine's own stream); the call
+ * returns once the work is enqueued. Without it, the call is synchronous.
+ * No counterpart in the reference, which processes one clip per call. */
+HV_API int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
+                     double f0_floor, double f0_ceil, double frame_period, int device,
+                     double* f0, double* times, unsigned flags, void* stream);
+
+/* Like hv_harvest, also reporting per-stage device milliseconds into
+ * stage_ms[HV_STAGE_COUNT] (reference _profile, src/bindings.cpp:90-104). */
+#define HV_STAGE_COUNT 6
+HV_API const char* hv_stage_name(int stage);
+HV_API int hv_profile(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil,
+               double frame_period, int device, double* f0, double* times, int64_t out_len,
+               double* stage_ms);
+
+/* Diagnostic: runs hv_harvest on one clip and copies the intermediate stage
+ * buffers to host memory, for stage-by-stage parity tests. Any pointer may
+ * be NULL. Shapes (row-major, frames = analysis frames on the 1 ms grid,
+ * cap = 7 * round(bands / 10)): y[y_len] decimated and DC-free waveform;
+ * raw[bands * frames] per-band candidates; count[1] candidates per frame;
+ * cand[frames * cap/7] candidates before overlap; refined, scores, pruned,
+ * pruned_scores[frames * cap]; best[frames]; smoothed[frames]. Mirrors the
+ * reference's stage split of src/engine.cpp:292-326. */
+HV_API int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil,
+                             int device, double* y, double* raw, int* count, double* cand,
+                             double* refined, double* scores, double* pruned,
+                             double* pruned_scores, double* best, double* smoothed);
+
+/* Releases cached device and host working memory on every device.
+ * Workspaces in use finish their call first (reference bindings.cpp:60-65,
+ * src/workspace_cache.h:61-70). */
+HV_API int hv_clear_cache(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HARVEST_B200_H_ */

@@ -1,0 +1,128 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes front end for the two CPU checkers.
+
+* ``port()``: the C restatement in ``harvest_oracle.c`` (``liboracle.so``).
+* ``reference()``: the reference's own bundled WORLD Harvest compiled from the
+  reference sources by ``Makefile`` into ``_ref/libworld_ref.so``; ``None``
+  when that library was never built.
+
+Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this package, and only as the checker or the timed CPU
+baseline. The engine under ``harvest_cuda_b200`` never does.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_LIB = os.path.join(HERE, "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libworld_ref.so")
+
+_D = ct.POINTER(ct.c_double)
+_I = ct.POINTER(ct.c_int)
+
+
+def build(quiet=True):
+    """Compile both checkers (the reference one only where its tree exists)."""
+    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+    if not quiet:
+        print(out.stdout)
+
+
+def _ptr(a, kind=_D):
+    return a.ctypes.data_as(kind)
+
+
+class Checker:
+    """One CPU implementation of Harvest with stage dumps."""
+
+    def __init__(self, path, name):
+        self.name = name
+        self.lib = ct.CDLL(path)
+        lib = self.lib
+        lib.oracle_params.argtypes = [ct.c_int, ct.c_int, ct.c_double, ct.c_double, _I]
+        lib.oracle_output_length.argtypes = [ct.c_int, ct.c_int, ct.c_double]
+        lib.oracle_output_length.restype = ct.c_int
+        lib.oracle_harvest.argtypes = [_D, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                       ct.c_double, _D, _D]
+        lib.oracle_stages.argtypes = [_D, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                      _D, _D, _I, _D, _D, _D, _D, _D, _D, _D, _D]
+        lib.oracle_fix_contour.argtypes = [_D, _D, ct.c_int, ct.c_int, ct.c_int, _D]
+        lib.oracle_smooth_contour.argtypes = [_D, ct.c_int, _D]
+
+    def params(self, n, fs, f0_floor=71.0, f0_ceil=800.0):
+        out = np.zeros(6, dtype=np.int32)
+        self.lib.oracle_params(int(n), int(fs), float(f0_floor), float(f0_ceil), _ptr(out, _I))
+        keys = ("ratio", "y_len", "fft_size", "bands", "frames", "capacity")
+        return {k: int(v) for k, v in zip(keys, out)}
+
+    def harvest(self, x, fs, f0_floor=71.0, f0_ceil=800.0, frame_period=5.0):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        m = self.lib.oracle_output_length(len(x), int(fs), float(frame_period))
+        f0 = np.zeros(m)
+        t = np.zeros(m)
+        self.lib.oracle_harvest(_ptr(x), len(x), int(fs), float(f0_floor), float(f0_ceil),
+                                float(frame_period), _ptr(t), _ptr(f0))
+        return f0, t
+
+    def stages(self, x, fs, f0_floor=71.0, f0_ceil=800.0):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        p = self.params(len(x), fs, f0_floor, f0_ceil)
+        fr, cap = p["frames"], p["capacity"]
+        out = dict(
+            y=np.zeros(p["y_len"]), raw=np.zeros((p["bands"], fr)),
+            cand=np.zeros((fr, cap)), refined=np.zeros((fr, cap)), scores=np.zeros((fr, cap)),
+            pruned=np.zeros((fr, cap)), pruned_scores=np.zeros((fr, cap)),
+            base=np.zeros(fr), fixed=np.zeros(fr), smoothed=np.zeros(fr))
+        count = np.zeros(1, dtype=np.int32)
+        self.lib.oracle_stages(
+            _ptr(x), len(x), int(fs), float(f0_floor), float(f0_ceil), _ptr(out["y"]),
+            _ptr(out["raw"]), _ptr(count, _I), _ptr(out["cand"]), _ptr(out["refined"]),
+            _ptr(out["scores"]), _ptr(out["pruned"]), _ptr(out["pruned_scores"]),
+            _ptr(out["base"]), _ptr(out["fixed"]), _ptr(out["smoothed"]))
+        out["count"] = int(count[0])
+        out["params"] = p
+        return out
+
+    def fix_contour(self, cand, scores, columns=None):
+        cand = np.ascontiguousarray(cand, dtype=np.float64)
+        scores = np.ascontiguousarray(scores, dtype=np.float64)
+        frames, stride = cand.shape
+        out = np.zeros(frames)
+        self.lib.oracle_fix_contour(_ptr(cand), _ptr(scores), frames,
+                                    stride if columns is None else int(columns), stride,
+                                    _ptr(out))
+        return out
+
+    def smooth_contour(self, f0):
+        f0 = np.ascontiguousarray(f0, dtype=np.float64)
+        out = np.zeros(len(f0))
+        self.lib.oracle_smooth_contour(_ptr(f0), len(f0), _ptr(out))
+        return out
+
+
+_cache = {}
+
+
+def port():
+    if "port" not in _cache:
+        if not os.path.exists(PORT_LIB):
+            build()
+        _cache["port"] = Checker(PORT_LIB, "port")
+    return _cache["port"]
+
+
+def reference():
+    if "ref" not in _cache:
+        _cache["ref"] = Checker(REF_LIB, "reference") if os.path.exists(REF_LIB) else None
+    return _cache["ref"]
+
+
+def best():
+    """The reference build when present, else the restatement."""
+    return reference() or port()
