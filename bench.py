@@ -1,0 +1,469 @@
+"""Throughput benchmark of the Harvest engine (one JSON line on rank 0).
+
+Workload (default): the ragged batch of 256 clips at 16 kHz, lengths
+uniform 1-12 s (about 1.7k audio seconds), floor 50 Hz, ceil 1100 Hz,
+frame_period 5 ms; synthetic seeded glide clips (F0 100 -> 250 Hz, 10
+harmonics, 20 dB SNR, 0.3 s unvoiced noise at both ends). A step is one
+pass of the whole Harvest pipeline over that batch.
+
+* ``value``: audio seconds per second with the batch resident in HBM,
+  through the C ABI with device pointers (one replayed CUDA graph per step),
+  timed with CUDA events on the launching stream; max over ranks.
+* ``e2e``: the same metric through the public NumPy API
+  (``harvest_batch``): host-to-device copy of the step's input from pinned
+  memory, compute, device-to-host copy of f0 and times, per step.
+* ``per_clip``: the plain per-clip path (``harvest`` once per clip).
+* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
+  CUDA-event duration (stage-timed steps) against the measured HBM copy
+  bandwidth, plus its algorithmic FP64 FLOP rate against the measured FP64
+  FMA peak.
+* ``cpu_baseline``: the reference's bundled WORLD Harvest (oracle/_ref) on
+  the host cores over a bounded sample of the same batch.
+
+``--impl reference`` times that CPU implementation alone on the host cores
+and prints the same line with ``"impl": "reference"``.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (fs, floor, ceil, period, description)
+    "batch256_16k": "256 clips x U(1,12) s at 16 kHz, floor 50, ceil 1100, period 5 ms",
+    "batch64_48k": "64 clips x U(2,30) s at 48 kHz, floor 71, ceil 800, period 1 ms",
+    "clip60s_44k": "1 clip of 60 s at 44.1 kHz, floor 71, ceil 800, period 5 ms",
+    "clip3s_16k": "1 clip of 3 s at 16 kHz, floor 71, ceil 800, period 5 ms",
+}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="batch256_16k")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="target duration of the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-per-clip", action="store_true")
+    return ap.parse_args()
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- models --
+LN2 = 0.69314718055994529
+
+
+def clip_params(n, fs, floor, ceil):
+    """Per-clip analysis sizes (reference src/engine.cpp:255-266)."""
+    ratio = min(12, max(1, int(fs / 8000.0 + 0.5)))
+    fs_r = fs / ratio
+    lo, hi = floor * 0.9, ceil * 1.1
+    bands = 1 + int(math.log(hi / lo) / LN2 * 40.0)
+    y_len = -(-n // ratio)
+    first = lo * 2.0 ** (1 / 40.0)
+    m = y_len + 5 + 2 * int(2.0 * fs_r / first)
+    nfft = int(2.0 ** (int(math.log(m) / LN2) + 1.0))
+    frames = int(1000.0 * n / fs) + 1
+    return dict(ratio=ratio, bands=bands, y_len=y_len, nfft=nfft, frames=frames,
+                capacity=7 * int(bands / 10.0 + 0.5))
+
+
+def band_bank_models(lengths, fs, floor, ceil):
+    """Algorithmic bytes and FP64 FLOPs of the band-pass bank stage for a
+    batch: per clip, the filtered band signals written and read once
+    (16 B x bands x y_len) plus the per-band candidates (16 B x bands x
+    frames); FLOPs of one n-point real inverse FFT and spectrum product per
+    band, 2.5 n log2 n + 6 (n/2 + 1), with the filter spectra cached."""
+    nbytes = flops = 0.0
+    for n in lengths:
+        p = clip_params(int(n), fs, floor, ceil)
+        nbytes += 16.0 * p["bands"] * p["y_len"] + 16.0 * p["bands"] * p["frames"]
+        nf = p["nfft"]
+        flops += p["bands"] * (2.5 * nf * math.log2(nf) + 6.0 * (nf / 2 + 1))
+    return nbytes, flops
+
+
+def byte_model(lengths, fs, floor, ceil, period):
+    """Stage-boundary byte model of the whole pipeline per batch."""
+    total = 0.0
+    for n in lengths:
+        p = clip_params(int(n), fs, floor, ceil)
+        out = int(1000.0 * n / fs / period) + 1
+        total += (8.0 * n + 16.0 * p["y_len"] + 16.0 * p["bands"] * p["y_len"]
+                  + 16.0 * p["bands"] * p["frames"] + 32.0 * p["frames"] * p["capacity"]
+                  + 16.0 * out)
+    return total
+
+
+# ------------------------------------------------------------- workloads --
+def make_workload(name, seed):
+    from harvest_cuda_b200 import signals
+    wl = signals.workload(name, seed=seed)
+    packed, offsets = signals.pack(wl["clips"])
+    return dict(packed=packed, offsets=offsets, fs=wl["fs"], floor=wl["f0_floor"],
+                ceil=wl["f0_ceil"], period=wl["frame_period"],
+                lengths=np.diff(offsets).tolist())
+
+
+# --------------------------------------------------------------- clocks --
+CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+
+class ClockSampler:
+    """Samples nvidia-smi every 200 ms while the timed region runs."""
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={CLOCK_QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], None, set()
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------- CPU baseline --
+def _world_clip(args):
+    x, fs, floor, ceil, period = args
+    import oracle
+    checker = oracle.best()
+    t0 = time.perf_counter()
+    checker.harvest(x, fs, floor, ceil, period)
+    return time.perf_counter() - t0, checker.name
+
+
+def cpu_sample(wl, target_seconds, cores):
+    """Clips of the workload whose CPU time is about target_seconds on
+    `cores` cores, at about 2.5 audio-s/s per core (floor 50 Hz, 190 bands)."""
+    budget = target_seconds * cores * 2.5 * wl["fs"]
+    chosen, total = [], 0
+    offs = wl["offsets"]
+    for i in range(len(offs) - 1):
+        n = int(offs[i + 1] - offs[i])
+        if total + n > budget and chosen:
+            break
+        chosen.append(i)
+        total += n
+    return chosen
+
+
+def run_cpu(pool, wl, clips):
+    offs, x = wl["offsets"], wl["packed"]
+    tasks = [(np.ascontiguousarray(x[offs[i]:offs[i + 1]]), wl["fs"], wl["floor"], wl["ceil"],
+              wl["period"]) for i in clips]
+    t0 = time.perf_counter()
+    results = pool.map(_world_clip, tasks, chunksize=1)
+    wall = time.perf_counter() - t0
+    audio = sum(t[0].size for t in tasks) / wl["fs"]
+    kind = "reference" if results and results[0][1] == "reference" else "port"
+    return audio, wall, kind
+
+
+def kernels_per_step(ratio):
+    # decimation (3 kernels per direction, or one copy at ratio 1), mean and
+    # edge bins, band bank, candidates, refinement, prune + best, contour.
+    return (6 if ratio > 1 else 1) + 1 + 1 + 1 + 1 + 2 + 1
+
+
+def fp64_peak(device):
+    import ctypes as ct
+    path = os.path.join(ROOT, "harvest_cuda_b200", "libhv_peaks.so")
+    if not os.path.exists(path):
+        return None
+    lib = ct.CDLL(path)
+    out = ct.c_double(0.0)
+    if lib.hv_peak_fp64(int(device), ct.byref(out)) != 0:
+        return None
+    return out.value
+
+
+# ------------------------------------------------------ reference arm --
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    wl = make_workload(args.workload, seed=1000)
+    pool = mp.get_context("spawn").Pool(cores)
+    per_step = max(2.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
+    clips = cpu_sample(wl, per_step, cores)
+    audio_total = wall_total = 0.0
+    kind = "port"
+    for step in range(args.warmup + args.steps):
+        audio, wall, kind = run_cpu(pool, wl, clips)
+        if step >= args.warmup:
+            audio_total += audio
+            wall_total += wall
+    pool.close()
+    value = audio_total / wall_total
+    line = {
+        "impl": "reference", "metric": "batched audio-s/s (16 kHz)", "value": value,
+        "unit": "audio-s/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * wall_total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                   "sample_clips": len(clips)},
+        "cpu_baseline": {"value": value, "unit": "audio-s/s", "cores": cores, "kind": kind,
+                         "sample": f"{len(clips)} clips ({audio_total / args.steps:.1f} audio-s) "
+                                   f"of the workload per step, one clip per worker process"},
+        "e2e": {"value": value, "unit": "audio-s/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------ our arm --
+def run_ours(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    cores = os.cpu_count() or 1
+    # The CPU pool starts before any GPU call (spawned workers).
+    pool = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        pool = mp.get_context("spawn").Pool(cores)
+    wl = make_workload(args.workload, seed=1000 + rank)
+
+    import datetime
+    import ctypes as ct
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    import harvest_cuda_b200 as hv
+    from harvest_cuda_b200 import _native
+
+    fs, floor, ceil, period = wl["fs"], wl["floor"], wl["ceil"], wl["period"]
+    offsets = np.ascontiguousarray(wl["offsets"], dtype=np.int64)
+    clips = offsets.size - 1
+    audio = float(offsets[-1]) / fs
+    out_off = hv.api._out_offsets(offsets, fs, period)
+    x_dev = torch.from_numpy(wl["packed"]).to(f"cuda:{local}")
+    f0_dev = torch.empty(int(out_off[-1]), dtype=torch.float64, device=f"cuda:{local}")
+    t_dev = torch.empty_like(f0_dev)
+    # A dedicated stream: torch's default is the legacy NULL stream, which the
+    # C ABI maps to the engine's own stream.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    off_ptr = offsets.ctypes.data_as(ct.POINTER(ct.c_int64))
+
+    def device_step(flags=0):
+        status = _native.lib.hv_harvest_batch(
+            x_dev.data_ptr(), off_ptr, clips, fs, floor, ceil, period, local, f0_dev.data_ptr(),
+            t_dev.data_ptr(), _native.HV_DEVICE_POINTERS | flags, stream.cuda_stream)
+        _native.raise_for(status)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # --- value: device-resident batch, replayed graph, CUDA events.
+    for _ in range(max(3, args.warmup)):
+        device_step()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            device_step()
+        end.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(start.elapsed_time(end) / args.steps)
+    value = audio * world / (ms / 1000.0)
+
+    # --- stage-timed steps: per-stage CUDA events on the same stream.
+    stage_steps = max(3, min(args.steps, 5))
+    acc = np.zeros(_native.HV_STAGE_COUNT)
+    buf = np.zeros(_native.HV_STAGE_COUNT)
+    for _ in range(stage_steps):
+        device_step(_native.HV_RECORD_STAGES)
+        _native.raise_for(_native.lib.hv_last_stage_ms(buf.ctypes.data_as(ct.POINTER(ct.c_double))))
+        acc += buf
+    stage_ms = acc / stage_steps
+    names = [_native.lib.hv_stage_name(i).decode() for i in range(_native.HV_STAGE_COUNT)]
+    stages = dict(zip(names, stage_ms.round(4).tolist()))
+
+    # --- e2e: public NumPy API from pinned host memory.
+    pinned = torch.from_numpy(wl["packed"]).pin_memory()
+    x_host = pinned.numpy()
+    hv.harvest_batch(x_host, offsets, fs, floor, ceil, period, device=local)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        f0, times, _ = hv.harvest_batch(x_host, offsets, fs, floor, ceil, period, device=local)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+    barrier()
+    e2e = {"value": audio * world / e2e_s, "unit": "audio-s/s",
+           "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(f0.nbytes + times.nbytes)}
+
+    line = None
+    if rank == 0:
+        line = summarize(args, wl, value, ms, stages, e2e, clocks.summary(), local, world)
+        if world == 1 and not args.no_per_clip:
+            line["per_clip"] = per_clip(hv, wl, local)
+            line["batched_over_per_clip"] = round(e2e["value"] / line["per_clip"]["value"], 2)
+        if pool is not None:
+            sample = cpu_sample(wl, args.cpu_seconds, cores)
+            a, wall, kind = run_cpu(pool, wl, sample)
+            pool.close()
+            line["cpu_baseline"] = {
+                "value": a / wall, "unit": "audio-s/s", "cores": cores, "kind": kind,
+                "sample": f"{len(sample)} of the batch's clips ({a:.1f} audio-s), one clip per "
+                          f"worker process, {wall:.1f} s wall"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def stage_models(wl):
+    """Algorithmic bytes (and FP64 FLOPs where a model exists) per stage for
+    one pass over the batch, from the stage-boundary byte model."""
+    fs, floor, ceil, period = wl["fs"], wl["floor"], wl["ceil"], wl["period"]
+    models = {k: [0.0, None] for k in
+              ("decimate", "band_bank", "candidates", "refine", "prune", "contour")}
+    for n in wl["lengths"]:
+        p = clip_params(int(n), fs, floor, ceil)
+        fr, cap, bands = p["frames"], p["capacity"], p["bands"]
+        out = int(1000.0 * n / fs / period) + 1
+        models["decimate"][0] += 8.0 * n + 16.0 * p["y_len"]
+        models["candidates"][0] += 8.0 * bands * fr + 8.0 * fr * cap / 7
+        models["refine"][0] += 8.0 * fr * cap / 7 + 32.0 * fr * cap
+        models["prune"][0] += 64.0 * fr * cap
+        models["contour"][0] += 32.0 * fr * cap + 16.0 * out
+    nbytes, flops = band_bank_models(wl["lengths"], fs, floor, ceil)
+    models["band_bank"] = [nbytes, flops]
+    return models
+
+
+def summarize(args, wl, value, ms, stages, e2e, clocks, device, world):
+    hbm, hbm_src = load_peaks()
+    models = stage_models(wl)
+    dominant = max(stages, key=stages.get)
+    nbytes, flops = models[dominant]
+    dur = stages[dominant] / 1000.0
+    roof = {"bound": "hbm", "kernel": dominant, "achieved": nbytes / dur / 1e9, "peak": hbm,
+            "unit": "GB/s", "frac": nbytes / dur / 1e9 / hbm, "traffic": None,
+            "peak_source": hbm_src, "algorithmic_bytes": nbytes, "launch_ms": stages[dominant]}
+    peak64 = fp64_peak(device)
+    if flops is not None and peak64:
+        roof["fp64"] = {"achieved": flops / dur / 1e12, "peak": peak64, "unit": "TFLOP/s",
+                        "frac": flops / dur / 1e12 / peak64, "algorithmic_flops": flops,
+                        "peak_source": "measured FMA loop (libhv_peaks)"}
+    ratio = clip_params(int(wl["lengths"][0]), wl["fs"], wl["floor"], wl["ceil"])["ratio"]
+    return {
+        "metric": "batched audio-s/s (16 kHz)", "value": value, "unit": "audio-s/s",
+        "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
+                   "clips_per_gpu": len(wl["lengths"]),
+                   "audio_seconds_per_gpu": float(sum(wl["lengths"])) / wl["fs"],
+                   "l2": "inputs and working set larger than L2 (no flush)",
+                   "parallelism": f"clip sharding, {world} GPU(s), no collective"},
+        "stage_ms": stages, "roofline": roof, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": kernels_per_step(ratio) * args.steps,
+        "model_bytes_per_step": byte_model(wl["lengths"], wl["fs"], wl["floor"], wl["ceil"],
+                                           wl["period"]),
+    }
+
+
+def per_clip(hv, wl, device):
+    """The plain per-clip path: harvest() once per clip, host buffers."""
+    offs, x = wl["offsets"], wl["packed"]
+    clips = [np.ascontiguousarray(x[offs[i]:offs[i + 1]]) for i in range(len(offs) - 1)]
+    for c in clips[:4]:
+        hv.harvest(c, wl["fs"], wl["floor"], wl["ceil"], wl["period"], device=device)
+    t0 = time.perf_counter()
+    for c in clips:
+        hv.harvest(c, wl["fs"], wl["floor"], wl["ceil"], wl["period"], device=device)
+    wall = time.perf_counter() - t0
+    audio = float(offs[-1]) / wl["fs"]
+    return {"value": audio / wall, "unit": "audio-s/s", "ms_per_pass": 1000.0 * wall}
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -15,6 +15,7 @@ HV_INVALID_ARGUMENT = 1
 HV_RUNTIME_ERROR = 2
 HV_DEVICE_POINTERS = 1
 HV_NO_GRAPH = 2
+HV_RECORD_STAGES = 4
 HV_STAGE_COUNT = 6
 
 _D = ct.POINTER(ct.c_double)
@@ -33,6 +34,7 @@ SIGNATURES = {
                                     ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_uint,
                                     ct.c_void_p]),
     "hv_stage_name": (ct.c_char_p, [ct.c_int]),
+    "hv_last_stage_ms": (ct.c_int, [_D]),
     "hv_profile": (ct.c_int, [_D, ct.c_int64, ct.c_int, ct.c_double, ct.c_double, ct.c_double,
                               ct.c_int, _D, _D, ct.c_int64, _D]),
     "hv_harvest_stages": (ct.c_int, [_D, ct.c_int64, ct.c_int, ct.c_double, ct.c_double, ct.c_int,

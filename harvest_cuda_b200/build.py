@@ -21,6 +21,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD_DIR = os.path.join(HERE, "_build")
 LIBRARY = os.path.join(HERE, "libharvest_b200.so")
+PEAKS_LIBRARY = os.path.join(HERE, "libhv_peaks.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["decimate.cu", "bandbank.cu", "candidates.cu", "contour.cu", "engine.cu"]
@@ -73,6 +74,13 @@ def build(force=False, verbose=False, ptxas_info=False):
         out = subprocess.run(cmd, capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + out.stdout + out.stderr)
+    # Measurement aid used by bench.py only (FP64 FMA peak).
+    peaks_src = os.path.join(CSRC, "peaks.cu")
+    if force or _stale(PEAKS_LIBRARY, [peaks_src]):
+        cmd = [nvcc(), *FLAGS, "-shared", peaks_src, "-o", PEAKS_LIBRARY]
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        if out.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + " ".join(cmd) + "\n" + out.stdout + out.stderr)
     return LIBRARY
 
 

@@ -32,6 +32,7 @@ namespace {
 
 // ---------------------------------------------------------------- errors --
 thread_local std::string g_error;
+thread_local double g_stage_ms[HV_STAGE_COUNT] = {};
 
 struct InvalidArgument : std::runtime_error { using std::runtime_error::runtime_error; };
 struct RuntimeFailure : std::runtime_error { using std::runtime_error::runtime_error; };
@@ -648,9 +649,18 @@ WorkspaceCache& cache() {
 
 const char* kStageNames[HV_STAGE_COUNT] = {"decimate", "band_bank", "candidates", "refine", "prune", "contour"};
 
+// Copies the stage intervals of the workspace's last recorded run.
+void collect_stage_ms(Workspace& ws) {
+  for (int i = 0; i < HV_STAGE_COUNT; ++i) {
+    float ms = 0;
+    check(cudaEventElapsedTime(&ms, ws.marks[i], ws.marks[i + 1]), "cudaEventElapsedTime");
+    g_stage_ms[i] = ms;
+  }
+}
+
 // Shared body of the host-pointer entry points.
 void run_host(const double* x, const int64_t* offsets, int clips, const Settings& s, int device,
-              double* f0, double* times, bool use_graph, double* stage_ms) {
+              double* f0, double* times, bool use_graph, bool record) {
   check_device(device);
   WorkspaceCache::Lease lease(cache(), device);
   Workspace& ws = lease.get();
@@ -661,7 +671,7 @@ void run_host(const double* x, const int64_t* offsets, int clips, const Settings
   check(cudaStreamWaitEvent(ws.stream, ws.last, 0), "cudaStreamWaitEvent");
   check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyHostToDevice, ws.stream),
         "cudaMemcpy(x)");
-  ws.run(p, ws.stream, use_graph, stage_ms != nullptr);
+  ws.run(p, ws.stream, use_graph, record);
   check(cudaMemcpyAsync(f0, ws.ptr<double>(p.at.f0), 8 * total_out, cudaMemcpyDeviceToHost, ws.stream),
         "cudaMemcpy(f0)");
   if (times)
@@ -669,12 +679,7 @@ void run_host(const double* x, const int64_t* offsets, int clips, const Settings
           "cudaMemcpy(times)");
   check(cudaEventRecord(ws.last, ws.stream), "cudaEventRecord");
   check(cudaStreamSynchronize(ws.stream), "harvest");
-  if (stage_ms)
-    for (int i = 0; i < HV_STAGE_COUNT; ++i) {
-      float ms = 0;
-      check(cudaEventElapsedTime(&ms, ws.marks[i], ws.marks[i + 1]), "cudaEventElapsedTime");
-      stage_ms[i] = ms;
-    }
+  if (record) collect_stage_ms(ws);
 }
 
 }  // namespace
@@ -719,7 +724,7 @@ int hv_harvest(const double* x, int64_t n, int fs, double f0_floor, double f0_ce
     validate_samples(x, n);
     if (out_len != samples_for(fs, n, frame_period)) throw InvalidArgument("output length mismatch");
     int64_t offsets[2] = {0, n};
-    run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, nullptr);
+    run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, false);
   });
 }
 
@@ -731,7 +736,15 @@ int hv_profile(const double* x, int64_t n, int fs, double f0_floor, double f0_ce
     validate_samples(x, n);
     if (out_len != samples_for(fs, n, frame_period)) throw InvalidArgument("output length mismatch");
     int64_t offsets[2] = {0, n};
-    run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, stage_ms);
+    run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, true);
+    std::memcpy(stage_ms, g_stage_ms, sizeof g_stage_ms);
+  });
+}
+
+int hv_last_stage_ms(double* stage_ms) {
+  return guarded([&] {
+    if (!stage_ms) throw InvalidArgument("null buffer");
+    std::memcpy(stage_ms, g_stage_ms, sizeof g_stage_ms);
   });
 }
 
@@ -750,10 +763,11 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
       validate_settings(offsets[c + 1] - offsets[c], fs, f0_floor, f0_ceil, frame_period);
     }
     Settings s{fs, f0_floor, f0_ceil, frame_period};
-    const bool use_graph = !(flags & HV_NO_GRAPH);
+    const bool record = (flags & HV_RECORD_STAGES) != 0;
+    const bool use_graph = !(flags & HV_NO_GRAPH) && !record;
     if (!(flags & HV_DEVICE_POINTERS)) {
       validate_samples(x + offsets[0], offsets[clips] - offsets[0]);
-      run_host(x, offsets, clips, s, device, f0, times, use_graph, nullptr);
+      run_host(x, offsets, clips, s, device, f0, times, use_graph, record);
       return;
     }
     check_device(device);
@@ -767,7 +781,7 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
     check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
     check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyDeviceToDevice, st),
           "cudaMemcpy(x)");
-    ws.run(p, st, use_graph, false);
+    ws.run(p, st, use_graph, record);
     check(cudaMemcpyAsync(f0, ws.ptr<double>(p.at.f0), 8 * total_out, cudaMemcpyDeviceToDevice, st),
           "cudaMemcpy(f0)");
     if (times)
@@ -776,6 +790,10 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
     // The workspace is reused by the next call on this device, on whatever
     // stream; that call waits for this event first.
     check(cudaEventRecord(ws.last, st), "cudaEventRecord");
+    if (record) {
+      check(cudaStreamSynchronize(st), "harvest_batch");
+      collect_stage_ms(ws);
+    }
   });
 }
 

@@ -36,6 +36,9 @@ extern "C" {
 /* Flags for hv_harvest_batch. */
 #define HV_DEVICE_POINTERS 1u /* x, f0 and times are device pointers on `device` */
 #define HV_NO_GRAPH 2u        /* launch stage by stage instead of replaying a CUDA graph */
+#define HV_RECORD_STAGES 4u   /* launch stage by stage with CUDA events between stages; the
+                                 call waits for the GPU and hv_last_stage_ms() returns the
+                                 per-stage device milliseconds of this call */
 
 /* Message describing the last failure on the calling thread ("" if none). */
 HV_API const char* hv_last_error(void);
@@ -77,6 +80,9 @@ HV_API int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, 
  * stage_ms[HV_STAGE_COUNT] (reference _profile, src/bindings.cpp:90-104). */
 #define HV_STAGE_COUNT 6
 HV_API const char* hv_stage_name(int stage);
+/* Per-stage device milliseconds of the calling thread's last call made with
+ * HV_RECORD_STAGES (or hv_profile) into stage_ms[HV_STAGE_COUNT]. */
+HV_API int hv_last_stage_ms(double* stage_ms);
 HV_API int hv_profile(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil,
                double frame_period, int device, double* f0, double* times, int64_t out_len,
                double* stage_ms);
