@@ -24,7 +24,7 @@ LIBRARY = os.path.join(HERE, "libharvest_b200.so")
 PEAKS_LIBRARY = os.path.join(HERE, "libhv_peaks.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["decimate.cu", "bandbank.cu", "candidates.cu", "contour.cu", "engine.cu"]
+SOURCES = ["decimate.cu", "bandbank.cu", "candidates.cu", "refine.cu", "contour.cu", "engine.cu"]
 HEADERS = ["hv_device.cuh", "hv_stages.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler",

@@ -279,7 +279,7 @@ struct Plan {
   void* meta = nullptr;
   size_t arena_bytes = 0;
   struct Layout {
-    size_t x, u, states, y, bins, queue, slots, raw, cand, count, refined, scores, pruned,
+    size_t x, u, states, y, bins, queue, slots, raw, cand, count, jobs, classes, refined, scores, pruned,
         pruned_scores, best, smoothed, scratch, f0, times;
   } at{};
   int bank_ctas = 0;
@@ -396,6 +396,8 @@ struct Workspace {
     p->bands = p->bank->bands;
     p->per_group = matlab_round_host(p->bands / 10.0);
     p->capacity = p->per_group * 7;
+    if (p->capacity >= kRefineColumns)
+      throw InvalidArgument("f0_floor/f0_ceil span too many band-pass channels");
     p->lag = static_cast<int>(std::ceil(140.0 / p->ratio) * p->ratio);
     const double first = p->bank->centre[0];
     p->x_off.assign(B + 1, 0); p->y_off.assign(B + 1, 0); p->t_off.assign(B + 1, 0);
@@ -494,6 +496,8 @@ struct Workspace {
     p->at.raw = take(8 * size_t(p->bands) * F);
     p->at.cand = take(8 * size_t(p->per_group) * F);
     p->at.count = take(4 * B);
+    p->at.jobs = take(sizeof(RefineJob) * size_t(p->capacity) * F);
+    p->at.classes = take(sizeof(int) * (2 * kRefineClasses + 1));
     p->at.refined = take(8 * size_t(p->capacity) * F);
     p->at.scores = take(8 * size_t(p->capacity) * F);
     p->at.pruned = take(8 * size_t(p->capacity) * F);
@@ -550,8 +554,13 @@ struct Workspace {
     check(launch_candidates(bv, ptr<double>(p.at.raw), F, ptr<double>(p.at.cand), ptr<int>(p.at.count), s),
           "candidates");
     mark(3);
-    check(launch_refine(bv, y, ptr<double>(p.at.cand), ptr<int>(p.at.count), F, ptr<double>(p.at.refined),
-                        ptr<double>(p.at.scores), s),
+    RefineBuffers rb{};
+    rb.class_count = ptr<int>(p.at.classes);
+    rb.class_cursor = rb.class_count + kRefineClasses;
+    rb.total = rb.class_cursor + kRefineClasses;
+    rb.jobs = ptr<RefineJob>(p.at.jobs);
+    check(launch_refine(bv, rb, y, ptr<double>(p.at.cand), ptr<int>(p.at.count), F,
+                        ptr<double>(p.at.refined), ptr<double>(p.at.scores), sms, s),
           "refine");
     mark(4);
     check(launch_prune(bv, ptr<double>(p.at.refined), ptr<double>(p.at.scores), ptr<int>(p.at.count), F,

@@ -61,9 +61,21 @@ cudaError_t launch_band_bank(const BankView& v, const double* y, const double* e
 
 cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t total_frames,
                               double* cand, int* count, cudaStream_t stream);
-cudaError_t launch_refine(const BatchView& v, const double* y, const double* cand,
-                          const int* count, int64_t total_frames, double* refined,
-                          double* scores, cudaStream_t stream);
+constexpr int kRefineClasses = 72;   // quarter-octave window-length classes
+constexpr int kRefineColumns = 1024; // job key = frame * kRefineColumns + column
+struct RefineJob {
+  double f0c;
+  long long key;
+};
+struct RefineBuffers {
+  int* class_count;    // [kRefineClasses]
+  int* class_cursor;   // [kRefineClasses]
+  int* total;          // [1]
+  RefineJob* jobs;     // [frames * capacity]
+};
+cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const double* y,
+                          const double* cand, const int* count, int64_t total_frames, double* refined,
+                          double* scores, int sms, cudaStream_t stream);
 cudaError_t launch_prune(const BatchView& v, const double* refined, const double* scores,
                          const int* count, int64_t total_frames, double* pruned,
                          double* pruned_scores, double* best, cudaStream_t stream);
