@@ -60,6 +60,8 @@ def parse_args():
                     help="target duration of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-clip", action="store_true")
+    ap.add_argument("--clips", type=int, default=0,
+                    help="use only the first N clips of the workload (small profiling runs)")
     return ap.parse_args()
 
 
@@ -119,9 +121,11 @@ def byte_model(lengths, fs, floor, ceil, period):
 
 
 # ------------------------------------------------------------- workloads --
-def make_workload(name, seed):
+def make_workload(name, seed, clips=0):
     from harvest_cuda_b200 import signals
     wl = signals.workload(name, seed=seed)
+    if clips:
+        wl["clips"] = wl["clips"][:clips]
     packed, offsets = signals.pack(wl["clips"])
     return dict(packed=packed, offsets=offsets, fs=wl["fs"], floor=wl["f0_floor"],
                 ceil=wl["f0_ceil"], period=wl["frame_period"],
@@ -244,7 +248,7 @@ def run_reference(args):
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    wl = make_workload(args.workload, seed=1000)
+    wl = make_workload(args.workload, seed=1000, clips=args.clips)
     pool = mp.get_context("spawn").Pool(cores)
     per_step = max(2.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
     clips = cpu_sample(wl, per_step, cores)
@@ -283,7 +287,7 @@ def run_ours(args):
     pool = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         pool = mp.get_context("spawn").Pool(cores)
-    wl = make_workload(args.workload, seed=1000 + rank)
+    wl = make_workload(args.workload, seed=1000 + rank, clips=args.clips)
 
     import datetime
     import ctypes as ct

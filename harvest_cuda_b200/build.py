@@ -24,8 +24,9 @@ LIBRARY = os.path.join(HERE, "libharvest_b200.so")
 PEAKS_LIBRARY = os.path.join(HERE, "libhv_peaks.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["decimate.cu", "bandbank.cu", "candidates.cu", "refine.cu", "contour.cu", "engine.cu"]
-HEADERS = ["hv_device.cuh", "hv_stages.cuh"]
+SOURCES = ["decimate.cu", "bandbank.cu", "bandbank_fft.cu", "candidates.cu", "refine.cu", "contour.cu",
+           "engine.cu"]
+HEADERS = ["hv_device.cuh", "hv_stages.cuh", "hv_events.cuh", "fft4096.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler",
                 "-fPIC,-ffp-contract=off,-fvisibility=hidden", "-I" + INCLUDE]

@@ -24,7 +24,7 @@
 // c1 = Q - P. The FIR computes the convolution divided by n (n is a power of
 // two, so the scale is exact and zero crossings are unchanged); the
 // correction is added divided by n as well.
-#include "hv_stages.cuh"
+#include "hv_events.cuh"
 
 namespace hv {
 
@@ -36,32 +36,6 @@ constexpr int kStep = kTile - 2;            // event positions per tile
 
 __device__ __forceinline__ int win_index(int j, int pitch) {
   return (j % kFirR) * pitch + j / kFirR;
-}
-
-// Sub-sample position of a negative-going crossing between s0 > 0 and
-// s1 <= 0 at integer edge e (harvest.cpp:184-186).
-__device__ __forceinline__ double fine_edge(int64_t e, double s0, double s1) {
-  return static_cast<double>(e) - s0 / (s1 - s0);
-}
-
-// Interval track k at time t: interp1 over (location, interval) pairs
-// derived from consecutive fine edges (harvest.cpp:188-191).
-__device__ double interval_at(const double* edges, int count, double fs, double t) {
-  // count edges -> count-1 intervals; location j = (e_j + e_{j+1}) / 2 / fs
-  int intervals = count - 1;
-  int lo = 0, hi = intervals;
-  while (lo < hi) {
-    int mid = (lo + hi) >> 1;
-    double loc = (edges[mid] + edges[mid + 1]) / 2.0 / fs;
-    if (loc <= t) lo = mid + 1; else hi = mid;
-  }
-  int seg = imin(imax(lo, 1), intervals - 1);
-  double x0 = (edges[seg - 1] + edges[seg]) / 2.0 / fs;
-  double x1 = (edges[seg] + edges[seg + 1]) / 2.0 / fs;
-  double y0 = fs / (edges[seg] - edges[seg - 1]);
-  double y1 = fs / (edges[seg + 1] - edges[seg]);
-  double s = (t - x0) / (x1 - x0);
-  return y0 + s * (y1 - y0);
 }
 
 // Exclusive block scan of four 16-bit counters packed in one 64-bit word.
@@ -92,7 +66,7 @@ band_bank_fir(BankView v, const double* __restrict__ y, const double* __restrict
   extern __shared__ double smem[];
   __shared__ unsigned long long scan_scratch[kBankThreads / 32];
   __shared__ int item_slot;
-  __shared__ double red[4][kBankThreads / 32];
+  __shared__ double red[3][kBankThreads / 32];
   const BatchView& B = v.batch;
   const int win_len = kTile + v.max_pad_taps + kFirR;
   const int pitch = (win_len + kFirR - 1) / kFirR + 1;
@@ -117,32 +91,9 @@ band_bank_fir(BankView v, const double* __restrict__ y, const double* __restrict
     const double* taps = v.taps_rev + v.tap_off[b];
     for (int i = tid; i < pad_taps; i += kBankThreads) s_taps[i] = taps[i];
 
-    // Final-bin correction constants for this (clip, band).
-    double hn = 0.0, hr = 0.0, hi = 0.0;
-    for (int m = tid; m <= 2 * half; m += kBankThreads) {
-      // taps_rev[j] = h[2 half - j]; h[m] = taps_rev[2 half - m]
-      double h = taps[2 * half - m];
-      double sg = (m & 1) ? -h : h;
-      double s, co;
-      sincospi(2.0 * m / n, &s, &co);
-      hn += sg; hr += sg * co; hi += sg * s;
-    }
-    for (int o = 16; o; o >>= 1) {
-      hn += __shfl_down_sync(0xffffffffu, hn, o);
-      hr += __shfl_down_sync(0xffffffffu, hr, o);
-      hi += __shfl_down_sync(0xffffffffu, hi, o);
-    }
-    if ((tid & 31) == 0) { red[0][tid >> 5] = hn; red[1][tid >> 5] = hr; red[2][tid >> 5] = hi; }
-    __syncthreads();
-    hn = hr = hi = 0.0;
-    for (int w = 0; w < kBankThreads / 32; ++w) { hn += red[0][w]; hr += red[1][w]; hi += red[2][w]; }
-    const double yn = edge_bins[3 * c], yr = edge_bins[3 * c + 1], yi = edge_bins[3 * c + 2];
-    // P = Y[n/2-1] * H[n/2-1], Q = Y[n/2] * P (harvest.cpp:123-128 order).
-    double pr = yr * hr - yi * hi, pi = yr * hi + yi * hr;
-    double qr = yn * pr, qi = yn * pi;
-    const double inv_n = 1.0 / n;
-    const double c0 = (qr - hn * yn) * inv_n;
-    const double c1r = (qr - pr) * inv_n, c1i = (qi - pi) * inv_n;
+    // Final-bin correction, divided by n like the FIR's convolution.
+    double c0, c1r, c1i;
+    final_bin_terms(taps, half, n, edge_bins + 3 * c, 1.0 / n, &red[0][0], c0, c1r, c1i);
 
     int count[4] = {0, 0, 0, 0};
     double* ev[4] = {events, events + v.slot_capacity, events + 2 * v.slot_capacity,
@@ -228,25 +179,8 @@ band_bank_fir(BankView v, const double* __restrict__ y, const double* __restrict
 
     // Interpolate the four interval tracks at every 1 ms frame.
     const int64_t f_begin = B.frame_off[c];
-    const int frames = static_cast<int>(B.frame_off[c + 1] - f_begin);
-    double* out = raw + b * v.total_frames + f_begin;
-    const bool usable = count[0] - 1 > 2 && count[1] - 1 > 2 && count[2] - 1 > 2 &&
-                        count[3] - 1 > 2;
-    const double centre = v.centre[b];
-    const double upper = centre * 1.1, lower = centre * 0.9;
-    for (int f = tid; f < frames; f += kBankThreads) {
-      double val = 0.0;
-      if (usable) {
-        double t = f * 1 / 1000.0;
-        double i0 = interval_at(ev[0], count[0], B.fs_r, t);
-        double i1 = interval_at(ev[1], count[1], B.fs_r, t);
-        double i2 = interval_at(ev[2], count[2], B.fs_r, t);
-        double i3 = interval_at(ev[3], count[3], B.fs_r, t);
-        val = (i0 + i1 + i2 + i3) / 4.0;
-        if (val > upper || val < lower || val > B.f0_ceil || val < B.f0_floor) val = 0.0;
-      }
-      out[f] = val;
-    }
+    band_contour(B, ev, count, v.centre[b], raw + b * v.total_frames + f_begin,
+                 static_cast<int>(B.frame_off[c + 1] - f_begin));
   }
 }
 

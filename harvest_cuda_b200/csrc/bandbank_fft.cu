@@ -1,0 +1,284 @@
+// a4-a9 by overlap-save FFT convolution: the band-pass bank, the four
+// interval detectors and the per-band candidates.
+//
+// WORLD filters every band with one whole-signal FFT of size n
+// (GetFilteredSignal, harvest.cpp:99-148). Here the convolution is split
+// into real blocks of B = 8192 samples that overlap by 2H + 2 (H the
+// largest filter half length), so every transform fits in shared memory:
+//   * block_spectra: the forward spectrum of every block of every clip,
+//     computed once and shared by all bands;
+//   * filter_spectra: per band the spectrum of its taps, placed so that the
+//     valid outputs of every band start at the same block offset 2H;
+//   * band_bank_fft: persistent CTAs take (clip, band) items longest first
+//     and walk the clip block by block: spectrum product, inverse transform,
+//     WORLD's final-bin correction, event detection and ordered compaction,
+//     then interp1 of the four interval tracks at every 1 ms frame.
+// The block outputs equal B times the linear convolution; WORLD's equal n
+// times it; both scales are powers of two, so zero crossings are unchanged
+// and the correction is added scaled by B / n.
+#include "fft4096.cuh"
+#include "hv_events.cuh"
+
+namespace hv {
+
+constexpr int kHalfN = kFftN;  // M: complex points per real block
+
+// tw[t] = e^{-2 pi i t / 8192}.
+__global__ void make_twiddles(double2* __restrict__ tw) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= kRealN) return;
+  double s, c;
+  sincospi(2.0 * t / kRealN, &s, &c);
+  tw[t] = make_double2(c, -s);
+}
+
+// Forward real FFT of the 8192 samples in `buf` (packed as z[m] = x[2m] +
+// i x[2m+1]) into spectrum[0..4096].
+__device__ void real_forward(double2* buf, const double2* __restrict__ tw, double2* __restrict__ out) {
+  __syncthreads();
+  fft4096<-1>(buf, tw);
+  for (int k = threadIdx.x; k <= kHalfN; k += kFftThreads) {
+    const double2 a = buf[fpad(k & (kHalfN - 1))];
+    const double2 b = conj2(buf[fpad((kHalfN - k) & (kHalfN - 1))]);
+    const double2 e = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
+    const double2 d = csub(a, b);
+    const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);  // d / (2i)
+    out[k] = cadd(e, cmul(twiddle<-1>(tw, k), o));
+  }
+}
+
+// One spectrum per block of every clip; block j of clip c holds
+// y[j V - H + 1 + p], p < 8192 (zero outside the clip).
+__global__ void __launch_bounds__(kFftThreads)
+block_spectra(BatchView v, FftBankGeometry g, const double* __restrict__ y,
+              const double2* __restrict__ tw, double2* __restrict__ spectra) {
+  extern __shared__ double2 buf[];
+  const int blk = blockIdx.x;
+  const int c = owner(g.blk_off, v.clips, blk);
+  const int64_t j = blk - g.blk_off[c];
+  const int64_t y0 = v.y_off[c];
+  const int64_t y_len = v.y_off[c + 1] - y0;
+  const int64_t start = j * g.valid - g.max_half + 1;
+  for (int m = threadIdx.x; m < kHalfN; m += kFftThreads) {
+    const int64_t p0 = start + 2 * m, p1 = p0 + 1;
+    buf[fpad(m)] = make_double2(p0 >= 0 && p0 < y_len ? y[y0 + p0] : 0.0,
+                                p1 >= 0 && p1 < y_len ? y[y0 + p1] : 0.0);
+  }
+  real_forward(buf, tw, spectra + static_cast<int64_t>(blk) * (kHalfN + 1));
+}
+
+// Per band the spectrum of g_b[p] = h_b[p - (H - h_b)], p in [H - h_b, H + h_b].
+__global__ void __launch_bounds__(kFftThreads)
+filter_spectra(const int* __restrict__ half, const int64_t* __restrict__ tap_off,
+               const double* __restrict__ taps_rev, int max_half, const double2* __restrict__ tw,
+               double2* __restrict__ filters) {
+  extern __shared__ double2 buf[];
+  const int b = blockIdx.x;
+  const int h = half[b];
+  const double* taps = taps_rev + tap_off[b];   // taps_rev[j] = h_b[2h - j]
+  auto tap = [&](int p) -> double {
+    const int m = p - (max_half - h);
+    return m >= 0 && m <= 2 * h ? taps[2 * h - m] : 0.0;
+  };
+  for (int m = threadIdx.x; m < kHalfN; m += kFftThreads) buf[fpad(m)] = make_double2(tap(2 * m), tap(2 * m + 1));
+  real_forward(buf, tw, filters + static_cast<int64_t>(b) * (kHalfN + 1));
+}
+
+// Event flags of the four kinds at position q of a block (harvest.cpp:162-238):
+// negative-going zero crossings of f, of -f, of the difference d[i] =
+// (-f[i]) - (-f[i+1]) and of -d, with their sub-sample edges.
+struct Events {
+  bool hit[4];
+  double fine[4];
+};
+
+__device__ __forceinline__ Events detect(const double* xs, int p, int64_t i, bool edge_ok, bool peak_ok) {
+  Events e{{false, false, false, false}, {0, 0, 0, 0}};
+  if (!edge_ok) return e;
+  const double f0 = xs[2 * fpad(p >> 1) + (p & 1)];
+  const double f1 = xs[2 * fpad((p + 1) >> 1) + ((p + 1) & 1)];
+  if (0.0 < f0 && f1 <= 0.0) { e.hit[0] = true; e.fine[0] = fine_edge(i + 1, f0, f1); }
+  const double a0 = -f0, a1 = -f1;
+  if (0.0 < a0 && a1 <= 0.0) { e.hit[1] = true; e.fine[1] = fine_edge(i + 1, a0, a1); }
+  if (peak_ok) {
+    const double f2 = xs[2 * fpad((p + 2) >> 1) + ((p + 2) & 1)];
+    const double a2 = -f2;
+    const double d0 = a0 - a1, d1 = a1 - a2;
+    if (0.0 < d0 && d1 <= 0.0) { e.hit[2] = true; e.fine[2] = fine_edge(i + 1, d0, d1); }
+    const double e0 = -d0, e1 = -d1;
+    if (0.0 < e0 && e1 <= 0.0) { e.hit[3] = true; e.fine[3] = fine_edge(i + 1, e0, e1); }
+  }
+  return e;
+}
+
+__global__ void __launch_bounds__(kFftThreads, 2)
+band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra,
+              const double2* __restrict__ filters, const double2* __restrict__ tw,
+              const double* __restrict__ edge_bins, int* __restrict__ queue, double* __restrict__ slots,
+              double* __restrict__ raw) {
+  extern __shared__ double2 buf[];
+  __shared__ int item_slot;
+  __shared__ double red[3 * (kFftThreads / 32)];
+  __shared__ int warp_count[kFftThreads / 32][4];
+  __shared__ int warp_base[kFftThreads / 32][4];
+  __shared__ int block_total[4];
+  __shared__ int chunk_bounds[8 * kFftThreads];
+  const BatchView& B = v.batch;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const unsigned below = (1u << lane) - 1;
+  double* xs = reinterpret_cast<double*>(buf);
+  double* events = slots + blockIdx.x * (4 * v.slot_capacity);
+  double* const ev[4] = {events, events + v.slot_capacity, events + 2 * v.slot_capacity,
+                         events + 3 * v.slot_capacity};
+  const int H = g.max_half;
+  for (;;) {
+    if (tid == 0) item_slot = atomicAdd(queue, 1);
+    __syncthreads();
+    const int item = item_slot;
+    __syncthreads();
+    if (item >= v.item_count) return;
+    const int c = v.items[item].x, b = v.items[item].y;
+    const int half = v.half[b];
+    const int64_t y_len = B.y_off[c + 1] - B.y_off[c];
+    const int n = B.nfft[c];
+    double c0, c1r, c1i;
+    final_bin_terms(v.taps_rev + v.tap_off[b], half, n, edge_bins + 3 * c,
+                    static_cast<double>(kRealN) / n, red, c0, c1r, c1i);
+    const double2* G = filters + static_cast<int64_t>(b) * (kHalfN + 1);
+    const int64_t blk0 = g.blk_off[c], blocks = g.blk_off[c + 1] - blk0;
+    // e^{-2 pi i 256 / n}: the step of this thread's correction phasor.
+    double step_s, step_c;
+    sincospi(2.0 * kFftThreads / n, &step_s, &step_c);
+    int count[4] = {0, 0, 0, 0};
+    for (int64_t j = 0; j < blocks; ++j) {
+      const double2* Y = spectra + (blk0 + j) * (kHalfN + 1);
+      __syncthreads();
+      // Spectrum product and packing for the inverse real transform:
+      // Z[k] = (X[k] + conj X[M-k]) + i e^{+2 pi i k / 8192} (X[k] - conj X[M-k]).
+      for (int k = tid; k <= kHalfN / 2; k += kFftThreads) {
+        const double2 xk = cmul(Y[k], G[k]);
+        const double2 xm = cmul(Y[kHalfN - k], G[kHalfN - k]);
+        const double2 w = twiddle<+1>(tw, k);
+        buf[fpad(k)] = cadd(cadd(xk, conj2(xm)), rot90<+1>(cmul(w, csub(xk, conj2(xm)))));
+        if (k != 0 && k != kHalfN / 2) {
+          const double2 w2 = make_double2(-w.x, w.y);   // e^{+2 pi i (M - k) / 8192}
+          buf[fpad(kHalfN - k)] = cadd(cadd(xm, conj2(xk)), rot90<+1>(cmul(w2, csub(xm, conj2(xk)))));
+        }
+      }
+      __syncthreads();
+      fft4096<+1>(buf, tw);
+      // Output i = j V + q sits at block sample p = 2H + q. Add WORLD's
+      // final-bin term at its unnormalised index i + half + 1.
+      const int64_t o = j * g.valid;
+      const int edge_end = static_cast<int>(min(static_cast<int64_t>(g.valid), y_len - 1 - o));
+      const int peak_end = static_cast<int>(min(static_cast<int64_t>(g.valid), y_len - 2 - o));
+      {
+        const int64_t q0 = o + half + 1 + tid;
+        double ps, pc;
+        sincospi(2.0 * static_cast<double>(q0 % n) / n, &ps, &pc);
+        for (int q = tid; q < edge_end + 2; q += kFftThreads) {
+          const int64_t qq = o + half + 1 + q;
+          const double corr = c0 + 2.0 * (c1r * pc + c1i * ps);
+          const int p = 2 * H + q;
+          xs[2 * fpad(p >> 1) + (p & 1)] += (qq & 1) ? -corr : corr;
+          const double nc = fma(pc, step_c, -ps * step_s);
+          ps = fma(pc, step_s, ps * step_c);
+          pc = nc;
+        }
+      }
+      __syncthreads();
+      // Ordered compaction, two passes: count per warp, then write.
+      const int per_warp = ((edge_end + kFftThreads / 32 - 1) / (kFftThreads / 32) + 31) & ~31;
+      const int q_begin = warp * per_warp, q_end = min(q_begin + per_warp, edge_end);
+      int mine[4] = {0, 0, 0, 0};
+      for (int q0 = q_begin; q0 < q_end; q0 += 32) {
+        const int q = q0 + lane;
+        const Events e = detect(xs, 2 * H + q, o + q, q < q_end, q < peak_end);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) mine[k] += __popc(__ballot_sync(0xffffffffu, e.hit[k]));
+      }
+      if (lane == 0)
+        for (int k = 0; k < 4; ++k) warp_count[warp][k] = mine[k];
+      __syncthreads();
+      if (tid < 4) {
+        int run = 0;
+        for (int w = 0; w < kFftThreads / 32; ++w) {
+          warp_base[w][tid] = run;
+          run += warp_count[w][tid];
+        }
+        block_total[tid] = run;
+      }
+      __syncthreads();
+      int at[4], added[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        at[k] = count[k] + warp_base[warp][k];
+        added[k] = block_total[k];
+      }
+      for (int q0 = q_begin; q0 < q_end; q0 += 32) {
+        const int q = q0 + lane;
+        const Events e = detect(xs, 2 * H + q, o + q, q < q_end, q < peak_end);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const unsigned m = __ballot_sync(0xffffffffu, e.hit[k]);
+          if (e.hit[k]) ev[k][at[k] + __popc(m & below)] = e.fine[k];
+          at[k] += __popc(m);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) count[k] += added[k];
+    }
+    __syncthreads();
+    const int64_t f_begin = B.frame_off[c];
+    band_contour_staged(B, ev, count, v.centre[b], raw + b * v.total_frames + f_begin,
+                        static_cast<int>(B.frame_off[c + 1] - f_begin), chunk_bounds, xs, 2 * kFftPadded);
+  }
+}
+
+// Host side --------------------------------------------------------------
+
+size_t fft_bank_smem_bytes() { return sizeof(double2) * kFftPadded; }
+
+int fft_bank_block_length() { return kRealN; }
+
+int fft_bank_ctas_per_sm() {
+  const size_t smem = fft_bank_smem_bytes();
+  if (cudaFuncSetAttribute(band_bank_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(block_spectra, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(filter_spectra, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)) !=
+          cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int blocks = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, band_bank_fft, kFftThreads, smem) != cudaSuccess)
+    blocks = 0;
+  cudaGetLastError();
+  return blocks;
+}
+
+cudaError_t launch_twiddles(double2* tw, cudaStream_t stream) {
+  make_twiddles<<<kRealN / 256, 256, 0, stream>>>(tw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_filter_spectra(const int* half, const int64_t* tap_off, const double* taps_rev, int bands,
+                                  int max_half, const double2* tw, double2* filters, cudaStream_t stream) {
+  filter_spectra<<<bands, kFftThreads, fft_bank_smem_bytes(), stream>>>(half, tap_off, taps_rev, max_half, tw,
+                                                                         filters);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fft_bank(const BankView& v, const FftBankGeometry& g, const double* y, const double* edge_bins,
+                            const double2* tw, const double2* filters, double2* spectra, int* queue,
+                            double* slots, int ctas, double* raw, cudaStream_t stream) {
+  block_spectra<<<static_cast<unsigned>(g.total_blocks), kFftThreads, fft_bank_smem_bytes(), stream>>>(
+      v.batch, g, y, tw, spectra);
+  band_bank_fft<<<ctas, kFftThreads, fft_bank_smem_bytes(), stream>>>(v, g, spectra, filters, tw, edge_bins,
+                                                                      queue, slots, raw);
+  return cudaGetLastError();
+}
+
+}  // namespace hv

@@ -34,54 +34,57 @@ __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
 }
 
 // a13: RemoveUnreliableCandidates(Sub) with SelectBestF0 (harvest.cpp:636-688)
-// and SearchF0Base (harvest.cpp:693-705). One thread per (frame, column)
-// writes the pruned pair; neighbours are read from the unpruned arrays.
-__global__ void prune_candidates(BatchView v, const double* __restrict__ refined,
-                                 const double* __restrict__ scores, const int* __restrict__ count,
-                                 int64_t total_frames, double* __restrict__ pruned,
-                                 double* __restrict__ pruned_scores) {
-  int64_t cell = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (cell >= total_frames * v.capacity) return;
-  int64_t gf = cell / v.capacity;
-  int col = static_cast<int>(cell - gf * v.capacity);
-  int c = owner(v.frame_off, v.clips, gf);
-  int64_t f0_row = v.frame_off[c];
-  int frames = static_cast<int>(v.frame_off[c + 1] - f0_row);
-  int f = static_cast<int>(gf - f0_row);
-  int columns = 7 * count[c];
-  double ref = refined[cell], sc = scores[cell];
-  if (col < columns && f >= 1 && f <= frames - 2 && ref != 0) {
-    double e1 = 1.0, e2 = 1.0;
-    const double* next = refined + (gf + 1) * v.capacity;
-    const double* prev = refined + (gf - 1) * v.capacity;
-    for (int j = 0; j < columns; ++j) {
-      double tmp = fabs(ref - next[j]) / ref;
-      if (!(tmp > e1)) e1 = tmp;
-    }
-    for (int j = 0; j < columns; ++j) {
-      double tmp = fabs(ref - prev[j]) / ref;
-      if (!(tmp > e2)) e2 = tmp;
-    }
-    double e = e1 < e2 ? e1 : e2;
-    if (!(e <= 0.05)) ref = sc = 0.0;
-  }
-  pruned[cell] = ref;
-  pruned_scores[cell] = sc;
-}
-
-__global__ void best_candidates(BatchView v, const double* __restrict__ pruned,
-                                const double* __restrict__ pruned_scores,
-                                const int* __restrict__ count, int64_t total_frames,
-                                double* __restrict__ best) {
-  int64_t gf = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+// and SearchF0Base (harvest.cpp:693-705). One warp per frame: lanes take
+// columns, neighbour rows are read from the unpruned arrays, and the best
+// candidate is the first column holding the highest pruned score.
+__global__ void __launch_bounds__(128)
+prune_frames(BatchView v, const double* __restrict__ refined, const double* __restrict__ scores,
+             const int* __restrict__ count, int64_t total_frames, double* __restrict__ pruned,
+             double* __restrict__ pruned_scores, double* __restrict__ best) {
+  const int lane = threadIdx.x & 31;
+  const int64_t gf = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
   if (gf >= total_frames) return;
-  int columns = 7 * count[owner(v.frame_off, v.clips, gf)];
+  const int c = owner(v.frame_off, v.clips, gf);
+  const int64_t row0 = v.frame_off[c];
+  const int frames = static_cast<int>(v.frame_off[c + 1] - row0);
+  const int f = static_cast<int>(gf - row0);
+  const int columns = 7 * count[c];
+  const int cap = v.capacity;
+  const double* row = refined + gf * cap;
+  const bool interior = f >= 1 && f <= frames - 2;
   double top = 0.0, pick = 0.0;
-  for (int j = 0; j < columns; ++j) {
-    double s = pruned_scores[gf * v.capacity + j];
-    if (s > top) { top = s; pick = pruned[gf * v.capacity + j]; }
+  int top_col = cap;
+  for (int col = lane; col < cap; col += 32) {
+    double ref = row[col], sc = scores[gf * cap + col];
+    if (col < columns && interior && ref != 0) {
+      const double* next = row + cap;
+      const double* prev = row - cap;
+      // SelectBestF0 leaves min(1, min_j |ref - c_j| / ref) as the error.
+      // Correctly rounded division by the same positive ref is monotone, so
+      // that equals the quotient of the smallest difference: one division
+      // per neighbour row, bit-identical.
+      double d1 = fabs(ref - next[0]), d2 = fabs(ref - prev[0]);
+      for (int j = 1; j < columns; ++j) {
+        d1 = fmin(d1, fabs(ref - next[j]));
+        d2 = fmin(d2, fabs(ref - prev[j]));
+      }
+      double e1 = d1 / ref, e2 = d2 / ref;
+      if (e1 > 1.0) e1 = 1.0;
+      if (e2 > 1.0) e2 = 1.0;
+      double e = e1 < e2 ? e1 : e2;
+      if (!(e <= 0.05)) ref = sc = 0.0;
+    }
+    pruned[gf * cap + col] = ref;
+    pruned_scores[gf * cap + col] = sc;
+    if (col < columns && sc > top) { top = sc; pick = ref; top_col = col; }
   }
-  best[gf] = pick;
+  for (int o = 16; o; o >>= 1) {
+    double ot = __shfl_down_sync(0xffffffffu, top, o);
+    double op = __shfl_down_sync(0xffffffffu, pick, o);
+    int oc = __shfl_down_sync(0xffffffffu, top_col, o);
+    if (ot > top || (ot == top && oc < top_col)) { top = ot; pick = op; top_col = oc; }
+  }
+  if (lane == 0) best[gf] = top > 0.0 ? pick : 0.0;
 }
 
 cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t total_frames,
@@ -95,12 +98,9 @@ cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t tot
 cudaError_t launch_prune(const BatchView& v, const double* refined, const double* scores,
                          const int* count, int64_t total_frames, double* pruned,
                          double* pruned_scores, double* best, cudaStream_t stream) {
-  const int threads = 128;
-  int64_t cells = total_frames * v.capacity;
-  prune_candidates<<<static_cast<unsigned>((cells + threads - 1) / threads), threads, 0, stream>>>(
-      v, refined, scores, count, total_frames, pruned, pruned_scores);
-  best_candidates<<<static_cast<unsigned>((total_frames + threads - 1) / threads), threads, 0,
-                    stream>>>(v, pruned, pruned_scores, count, total_frames, best);
+  const int warps = 4;
+  prune_frames<<<static_cast<unsigned>((total_frames + warps - 1) / warps), 32 * warps, 0, stream>>>(
+      v, refined, scores, count, total_frames, pruned, pruned_scores, best);
   return cudaGetLastError();
 }
 

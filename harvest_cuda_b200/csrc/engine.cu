@@ -15,6 +15,7 @@
 #include <atomic>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <list>
 #include <map>
@@ -227,7 +228,7 @@ struct Settings {
 // reversed, padded taps of GetFilteredSignal (harvest.cpp:101-108) computed
 // with the host's libm exactly as the reference does.
 struct BankTables {
-  int bands = 0, max_pad_taps = 0;
+  int bands = 0, max_pad_taps = 0, max_half = 0;
   std::vector<double> centre;
   std::vector<int> half;
   std::vector<int64_t> tap_off;
@@ -259,6 +260,7 @@ BankTables make_bank(int fs, double floor, double ceil) {
     t.centre.push_back(c);
     t.half.push_back(h);
     t.max_pad_taps = std::max(t.max_pad_taps, padded);
+    t.max_half = std::max(t.max_half, h);
   }
   return t;
 }
@@ -275,11 +277,18 @@ struct Plan {
   std::vector<int2> items;
   int64_t slot_capacity = 0, total_seg = 0;
   double trans[9];
+  // FFT band bank (overlap-save blocks), used unless the filters are too long.
+  bool use_fft = false;
+  int fft_valid = 0;
+  std::vector<int64_t> blk_off;
+  int64_t total_blocks = 0;
+  double2* filters = nullptr;  // [bands][4097] filter spectra (own allocation)
+  int64_t* d_blk_off = nullptr;
   // Device copy of all tables (one allocation) and arena layout.
   void* meta = nullptr;
   size_t arena_bytes = 0;
   struct Layout {
-    size_t x, u, states, y, bins, queue, slots, raw, cand, count, jobs, classes, refined, scores, pruned,
+    size_t x, u, states, y, bins, queue, slots, spectra, raw, cand, count, jobs, classes, refined, scores, pruned,
         pruned_scores, best, smoothed, scratch, f0, times;
   } at{};
   int bank_ctas = 0;
@@ -295,6 +304,7 @@ struct Plan {
   ~Plan() {
     if (graph) cudaGraphExecDestroy(graph);
     if (meta) cudaFree(meta);
+    if (filters) cudaFree(filters);
   }
 };
 
@@ -319,6 +329,7 @@ struct Workspace {
   void* arena = nullptr;
   size_t arena_size = 0;
   int sms = 0;
+  double2* twiddles = nullptr;  // e^{-2 pi i t / 8192}, t < 8192
   std::map<Settings, std::shared_ptr<const BankTables>> banks;
   std::list<std::unique_ptr<Plan>> plans;  // most recent first
 
@@ -328,6 +339,9 @@ struct Workspace {
     for (auto& e : marks) check(cudaEventCreate(&e), "cudaEventCreate");
     check(cudaEventCreateWithFlags(&last, cudaEventDisableTiming), "cudaEventCreate");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+    check(cudaMalloc(&twiddles, sizeof(double2) * fft_bank_block_length()), "cudaMalloc(twiddles)");
+    check(launch_twiddles(twiddles, stream), "twiddles");
+    check(cudaStreamSynchronize(stream), "twiddles");
   }
   ~Workspace() {
     try {
@@ -336,6 +350,7 @@ struct Workspace {
       if (stream) cudaStreamSynchronize(stream);
       plans.clear();
       if (arena) cudaFree(arena);
+      if (twiddles) cudaFree(twiddles);
       for (auto& e : marks) if (e) cudaEventDestroy(e);
       if (last) cudaEventDestroy(last);
       if (stream) cudaStreamDestroy(stream);
@@ -420,15 +435,33 @@ struct Workspace {
       p->slot_capacity = std::max<int64_t>(p->slot_capacity, y_len / 2 + 2);
     }
     p->total_seg = p->seg_off[B];
-    // Work items longest first.
     const BankTables& bank = *p->bank;
+    // The FFT bank needs its overlap (2 H + 2) to fit in half a block; the
+    // direct FIR covers longer filters. HARVEST_B200_BANK=fir|fft overrides.
+    const int block = fft_bank_block_length();
+    p->use_fft = 2 * bank.max_half + 2 <= block / 2;
+    if (const char* force = std::getenv("HARVEST_B200_BANK")) {
+      if (!std::strcmp(force, "fir")) p->use_fft = false;
+      if (!std::strcmp(force, "fft") && 2 * bank.max_half + 2 < block) p->use_fft = true;
+    }
+    p->blk_off.assign(B + 1, 0);
+    if (p->use_fft) {
+      p->fft_valid = block - 2 - 2 * bank.max_half;
+      for (int c = 0; c < B; ++c) {
+        int64_t positions = p->y_off[c + 1] - p->y_off[c] - 1;   // event positions 0..y_len-2
+        p->blk_off[c + 1] = p->blk_off[c] + (positions + p->fft_valid - 1) / p->fft_valid;
+      }
+      p->total_blocks = p->blk_off[B];
+    }
+    // Work items longest first.
     std::vector<std::pair<int64_t, int2>> items;
     items.reserve(size_t(B) * p->bands);
     for (int c = 0; c < B; ++c)
       for (int b = 0; b < p->bands; ++b) {
         int64_t y_len = p->y_off[c + 1] - p->y_off[c];
         int64_t taps = bank.tap_off[b + 1] - bank.tap_off[b];
-        items.push_back({y_len * (taps + 16), make_int2(c, b)});
+        int64_t cost = p->use_fft ? (p->blk_off[c + 1] - p->blk_off[c]) : y_len * (taps + 16);
+        items.push_back({cost, make_int2(c, b)});
       }
     std::stable_sort(items.begin(), items.end(),
                      [](const auto& a, const auto& b) { return a.first > b.first; });
@@ -462,6 +495,7 @@ struct Workspace {
     size_t o_h = put(bank.half.data(), 4 * bank.half.size());
     size_t o_to = put(bank.tap_off.data(), 8 * bank.tap_off.size());
     size_t o_tp = put(bank.taps_rev.data(), 8 * bank.taps_rev.size());
+    size_t o_bo = put(p->blk_off.data(), 8 * (B + 1));
     check(cudaMalloc(&p->meta, blob.size()), "cudaMalloc(plan)");
     check(cudaMemcpy(p->meta, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy(plan)");
     char* m = static_cast<char*>(p->meta);
@@ -478,8 +512,17 @@ struct Workspace {
     p->d_half = reinterpret_cast<int*>(m + o_h);
     p->d_tap_off = reinterpret_cast<int64_t*>(m + o_to);
     p->d_taps = reinterpret_cast<double*>(m + o_tp);
+    p->d_blk_off = reinterpret_cast<int64_t*>(m + o_bo);
+    if (p->use_fft) {
+      if (fft_bank_ctas_per_sm() < 1) throw RuntimeFailure("FFT band-bank kernel does not fit on this device");
+      check(cudaMalloc(&p->filters, sizeof(double2) * (block / 2 + 1) * bank.bands), "cudaMalloc(filters)");
+      check(launch_filter_spectra(p->d_half, p->d_tap_off, p->d_taps, bank.bands, bank.max_half, twiddles,
+                                  p->filters, stream),
+            "filter_spectra");
+      check(cudaStreamSynchronize(stream), "filter_spectra");
+    }
     // Arena layout.
-    int per_sm = band_bank_ctas_per_sm(bank.max_pad_taps);
+    int per_sm = p->use_fft ? fft_bank_ctas_per_sm() : band_bank_ctas_per_sm(bank.max_pad_taps);
     if (per_sm < 1) throw RuntimeFailure("band-bank kernel does not fit on this device");
     int items_n = static_cast<int>(p->items.size());
     p->bank_ctas = std::max(1, std::min(items_n, sms * per_sm));
@@ -493,6 +536,7 @@ struct Workspace {
     p->at.bins = take(8 * 3 * B);
     p->at.queue = take(16);
     p->at.slots = take(8 * 4 * p->slot_capacity * p->bank_ctas);
+    p->at.spectra = take(sizeof(double2) * (block / 2 + 1) * p->total_blocks);
     p->at.raw = take(8 * size_t(p->bands) * F);
     p->at.cand = take(8 * size_t(p->per_group) * F);
     p->at.count = take(4 * B);
@@ -546,9 +590,16 @@ struct Workspace {
     kv.items = p.d_items; kv.item_count = static_cast<int>(p.items.size());
     kv.max_pad_taps = p.bank->max_pad_taps; kv.total_frames = F; kv.slot_capacity = p.slot_capacity;
     check(cudaMemsetAsync(ptr<int>(p.at.queue), 0, 16, s), "memset");
-    check(launch_band_bank(kv, y, ptr<double>(p.at.bins), ptr<int>(p.at.queue), ptr<double>(p.at.slots),
-                           p.bank_ctas, ptr<double>(p.at.raw), s),
-          "band_bank");
+    if (p.use_fft) {
+      FftBankGeometry geo{p.bank->max_half, p.fft_valid, p.total_blocks, p.d_blk_off};
+      check(launch_fft_bank(kv, geo, y, ptr<double>(p.at.bins), twiddles, p.filters, ptr<double2>(p.at.spectra),
+                            ptr<int>(p.at.queue), ptr<double>(p.at.slots), p.bank_ctas, ptr<double>(p.at.raw), s),
+            "band_bank_fft");
+    } else {
+      check(launch_band_bank(kv, y, ptr<double>(p.at.bins), ptr<int>(p.at.queue), ptr<double>(p.at.slots),
+                             p.bank_ctas, ptr<double>(p.at.raw), s),
+            "band_bank");
+    }
     mark(2);
     check(cudaMemsetAsync(ptr<int>(p.at.count), 0, 4 * B, s), "memset");
     check(launch_candidates(bv, ptr<double>(p.at.raw), F, ptr<double>(p.at.cand), ptr<int>(p.at.count), s),

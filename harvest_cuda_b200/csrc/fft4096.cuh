@@ -1,0 +1,118 @@
+// 4096-point complex FP64 FFT in shared memory for one CTA of 256 threads:
+// three Stockham radix-16 passes, each thread holding one 16-point group in
+// registers. The buffer is padded by one element per 16 so the strided
+// stores of the first pass spread over the banks.
+//
+// Conventions: kSign = -1 computes X[k] = sum_m x[m] e^{-2 pi i m k / N};
+// kSign = +1 the unnormalised inverse. Twiddles come from a table
+// tw[t] = e^{-2 pi i t / 8192}, t in [0, 8192), shared with the real-FFT
+// packing of 8192-point real blocks.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace hv {
+
+constexpr int kFftN = 4096;          // complex points
+constexpr int kFftThreads = 256;
+constexpr int kRealN = 2 * kFftN;    // real block length
+constexpr int kFftPadded = kFftN + kFftN / 16;
+
+__device__ __forceinline__ int fpad(int i) { return i + (i >> 4); }
+
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 conj2(double2 a) { return make_double2(a.x, -a.y); }
+
+// e^{kSign 2 pi i t / 8192} from the table (which stores the minus sign).
+template <int kSign>
+__device__ __forceinline__ double2 twiddle(const double2* __restrict__ tw, int t) {
+  double2 w = tw[t & (kRealN - 1)];
+  return kSign < 0 ? w : conj2(w);
+}
+
+// Multiplication by kSign * i.
+template <int kSign>
+__device__ __forceinline__ double2 rot90(double2 a) {
+  return kSign < 0 ? make_double2(a.y, -a.x) : make_double2(-a.y, a.x);
+}
+
+template <int kSign>
+__device__ __forceinline__ void dft4(double2& a, double2& b, double2& c, double2& d) {
+  double2 t0 = cadd(a, c), t1 = csub(a, c), t2 = cadd(b, d), t3 = rot90<kSign>(csub(b, d));
+  a = cadd(t0, t2);
+  c = csub(t0, t2);
+  b = cadd(t1, t3);
+  d = csub(t1, t3);
+}
+
+// In-register 16-point DFT, x[n] -> X[k], as 4 x 4 with internal twiddles.
+template <int kSign>
+__device__ __forceinline__ void dft16(double2 (&x)[16]) {
+  const double c1 = 0.92387953251128675613, s1 = 0.38268343236508977173;  // cos, sin pi/8
+  const double r2 = 0.70710678118654752440;
+#pragma unroll
+  for (int n2 = 0; n2 < 4; ++n2) dft4<kSign>(x[n2], x[n2 + 4], x[n2 + 8], x[n2 + 12]);
+  // x[n2 + 4 k1] now holds A[n2][k1]; twiddle by e^{kSign 2 pi i n2 k1 / 16}.
+  const double2 w1 = make_double2(c1, kSign * s1), w2 = make_double2(r2, kSign * r2),
+                w3 = make_double2(s1, kSign * c1), w6 = make_double2(-r2, kSign * r2),
+                w9 = make_double2(-c1, -kSign * s1);
+  x[5] = cmul(x[5], w1);
+  x[6] = cmul(x[6], w2);
+  x[7] = cmul(x[7], w3);
+  x[9] = cmul(x[9], w2);
+  x[10] = rot90<kSign>(x[10]);
+  x[11] = cmul(x[11], w6);
+  x[13] = cmul(x[13], w3);
+  x[14] = cmul(x[14], w6);
+  x[15] = cmul(x[15], w9);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) dft4<kSign>(x[4 * k1], x[4 * k1 + 1], x[4 * k1 + 2], x[4 * k1 + 3]);
+  // X[k1 + 4 k2] sits at x[4 k1 + k2]: transpose the 4 x 4 index.
+  double2 t[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) t[i] = x[i];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) x[k1 + 4 * k2] = t[4 * k1 + k2];
+}
+
+// One Stockham pass with sub-transform length ls (1, 16, 256).
+template <int kSign>
+__device__ __forceinline__ void stockham_pass(double2* buf, const double2* __restrict__ tw, int ls) {
+  const int j = threadIdx.x;
+  const int k = j & (ls - 1);
+  double2 x[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) x[m] = buf[fpad(j + m * (kFftN / 16))];
+  if (ls > 1) {
+    // w = e^{kSign 2 pi i k / (16 ls)}; x[m] *= w^m.
+    const double2 w = twiddle<kSign>(tw, k * (kRealN / (16 * ls)));
+    double2 wm = w;
+#pragma unroll
+    for (int m = 1; m < 16; ++m) {
+      x[m] = cmul(x[m], wm);
+      wm = cmul(wm, w);
+    }
+  }
+  dft16<kSign>(x);
+  __syncthreads();
+  const int out0 = (j - k) * 16 + k;
+#pragma unroll
+  for (int m = 0; m < 16; ++m) buf[fpad(out0 + m * ls)] = x[m];
+  __syncthreads();
+}
+
+// Full transform of buf (natural order in and out). Callers synchronise
+// before the first pass; the last pass ends with a barrier.
+template <int kSign>
+__device__ __forceinline__ void fft4096(double2* buf, const double2* __restrict__ tw) {
+  stockham_pass<kSign>(buf, tw, 1);
+  stockham_pass<kSign>(buf, tw, 16);
+  stockham_pass<kSign>(buf, tw, 256);
+}
+
+}  // namespace hv

@@ -59,6 +59,24 @@ cudaError_t launch_band_bank(const BankView& v, const double* y, const double* e
                              int* queue, double* slots, int ctas, double* raw,
                              cudaStream_t stream);
 
+// Overlap-save geometry of the FFT band bank: real blocks of 8192 samples,
+// `valid` = 8192 - 2 - 2 max_half new outputs per block.
+struct FftBankGeometry {
+  int max_half;
+  int valid;
+  int64_t total_blocks;
+  const int64_t* blk_off;  // [clips + 1] block offsets
+};
+size_t fft_bank_smem_bytes();
+int fft_bank_block_length();
+int fft_bank_ctas_per_sm();
+cudaError_t launch_twiddles(double2* tw, cudaStream_t stream);
+cudaError_t launch_filter_spectra(const int* half, const int64_t* tap_off, const double* taps_rev, int bands,
+                                  int max_half, const double2* tw, double2* filters, cudaStream_t stream);
+cudaError_t launch_fft_bank(const BankView& v, const FftBankGeometry& g, const double* y, const double* edge_bins,
+                            const double2* tw, const double2* filters, double2* spectra, int* queue,
+                            double* slots, int ctas, double* raw, cudaStream_t stream);
+
 cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t total_frames,
                               double* cand, int* count, cudaStream_t stream);
 constexpr int kRefineClasses = 72;   // quarter-octave window-length classes

@@ -165,3 +165,19 @@ def test_deterministic(gpu):
         again = hv.harvest(x, 22050)
         np.testing.assert_array_equal(again[0], first[0])
         np.testing.assert_array_equal(again[1], first[1])
+
+
+def test_direct_fir_bank_matches_fft_bank(gpu, checker, monkeypatch):
+    # The engine picks the overlap-save FFT bank unless the filters are too
+    # long for it; force the direct FIR bank and compare both with the checker.
+    x = signals.kind_clip("speechlike", 1.3, 16000)
+    fft = hv.harvest(x, 16000)
+    monkeypatch.setenv("HARVEST_B200_BANK", "fir")
+    hv.clear_cache()
+    fir = hv.harvest(x, 16000)
+    monkeypatch.delenv("HARVEST_B200_BANK")
+    hv.clear_cache()
+    expected = checker.harvest(x, 16000)
+    for actual in (fft, fir):
+        np.testing.assert_array_equal(actual[1], expected[1])
+        np.testing.assert_allclose(actual[0], expected[0], rtol=1e-7, atol=1e-5)
