@@ -84,33 +84,6 @@ filter_spectra(const int* __restrict__ half, const int64_t* __restrict__ tap_off
   real_forward(buf, tw, filters + static_cast<int64_t>(b) * (kHalfN + 1));
 }
 
-// Event flags of the four kinds at position q of a block (harvest.cpp:162-238):
-// negative-going zero crossings of f, of -f, of the difference d[i] =
-// (-f[i]) - (-f[i+1]) and of -d, with their sub-sample edges.
-struct Events {
-  bool hit[4];
-  double fine[4];
-};
-
-__device__ __forceinline__ Events detect(const double* xs, int p, int64_t i, bool edge_ok, bool peak_ok) {
-  Events e{{false, false, false, false}, {0, 0, 0, 0}};
-  if (!edge_ok) return e;
-  const double f0 = xs[2 * fpad(p >> 1) + (p & 1)];
-  const double f1 = xs[2 * fpad((p + 1) >> 1) + ((p + 1) & 1)];
-  if (0.0 < f0 && f1 <= 0.0) { e.hit[0] = true; e.fine[0] = fine_edge(i + 1, f0, f1); }
-  const double a0 = -f0, a1 = -f1;
-  if (0.0 < a0 && a1 <= 0.0) { e.hit[1] = true; e.fine[1] = fine_edge(i + 1, a0, a1); }
-  if (peak_ok) {
-    const double f2 = xs[2 * fpad((p + 2) >> 1) + ((p + 2) & 1)];
-    const double a2 = -f2;
-    const double d0 = a0 - a1, d1 = a1 - a2;
-    if (0.0 < d0 && d1 <= 0.0) { e.hit[2] = true; e.fine[2] = fine_edge(i + 1, d0, d1); }
-    const double e0 = -d0, e1 = -d1;
-    if (0.0 < e0 && e1 <= 0.0) { e.hit[3] = true; e.fine[3] = fine_edge(i + 1, e0, e1); }
-  }
-  return e;
-}
-
 __global__ void __launch_bounds__(kFftThreads, 2)
 band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra,
               const double2* __restrict__ filters, const double2* __restrict__ tw,
@@ -119,18 +92,17 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
   extern __shared__ double2 buf[];
   __shared__ int item_slot;
   __shared__ double red[3 * (kFftThreads / 32)];
-  __shared__ int warp_count[kFftThreads / 32][4];
-  __shared__ int warp_base[kFftThreads / 32][4];
-  __shared__ int block_total[4];
+  __shared__ unsigned long long scan_scratch[kFftThreads / 32];
   __shared__ int chunk_bounds[8 * kFftThreads];
   const BatchView& B = v.batch;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const unsigned below = (1u << lane) - 1;
+  const int tid = threadIdx.x;
   double* xs = reinterpret_cast<double*>(buf);
   double* events = slots + blockIdx.x * (4 * v.slot_capacity);
   double* const ev[4] = {events, events + v.slot_capacity, events + 2 * v.slot_capacity,
                          events + 3 * v.slot_capacity};
   const int H = g.max_half;
+  const int run = g.run;   // positions per thread in the event scan (even)
+  const RunDivider div_run{run, 1.0f / run};
   for (;;) {
     if (tid == 0) item_slot = atomicAdd(queue, 1);
     __syncthreads();
@@ -166,9 +138,11 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
         }
       }
       __syncthreads();
-      fft4096<+1>(buf, tw);
-      // Output i = j V + q sits at block sample p = 2H + q. Add WORLD's
-      // final-bin term at its unnormalised index i + half + 1.
+      stockham_pass<+1>(buf, tw, 1);
+      stockham_pass<+1>(buf, tw, 16);
+      inverse_last_pass_to_runs(buf, tw, 2 * H, div_run);
+      // Output i = j V + q (block sample 2H + q) now sits at lin[q + q / run].
+      // Add WORLD's final-bin term at its unnormalised index i + half + 1.
       const int64_t o = j * g.valid;
       const int edge_end = static_cast<int>(min(static_cast<int64_t>(g.valid), y_len - 1 - o));
       const int peak_end = static_cast<int>(min(static_cast<int64_t>(g.valid), y_len - 2 - o));
@@ -179,54 +153,70 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
         for (int q = tid; q < edge_end + 2; q += kFftThreads) {
           const int64_t qq = o + half + 1 + q;
           const double corr = c0 + 2.0 * (c1r * pc + c1i * ps);
-          const int p = 2 * H + q;
-          xs[2 * fpad(p >> 1) + (p & 1)] += (qq & 1) ? -corr : corr;
+          xs[q + div_run(q)] += (qq & 1) ? -corr : corr;
           const double nc = fma(pc, step_c, -ps * step_s);
           ps = fma(pc, step_s, ps * step_c);
           pc = nc;
         }
       }
       __syncthreads();
-      // Ordered compaction, two passes: count per warp, then write.
-      const int per_warp = ((edge_end + kFftThreads / 32 - 1) / (kFftThreads / 32) + 31) & ~31;
-      const int q_begin = warp * per_warp, q_end = min(q_begin + per_warp, edge_end);
-      int mine[4] = {0, 0, 0, 0};
-      for (int q0 = q_begin; q0 < q_end; q0 += 32) {
-        const int q = q0 + lane;
-        const Events e = detect(xs, 2 * H + q, o + q, q < q_end, q < peak_end);
+      // Events: each thread scans a contiguous run of positions, counting in
+      // the first pass; a block scan of the packed counts orders the runs;
+      // the second pass writes the sub-sample edges of its hits.
+      const int q_lo = min(tid * run, edge_end), q_hi = min(q_lo + run, edge_end);
+      // Within this thread's run, sample q_lo + i sits at lin[q_lo + i + tid]
+      // (i < run) and the two lookahead samples one slot further.
+      const double* mine_lin = xs + q_lo + min(tid, edge_end / run + 1);
+      auto X = [&](int i) -> double { return mine_lin[i + (i >= run ? 1 : 0)]; };
+      const int len = q_hi - q_lo;
+      unsigned long long mine = 0;
+      for (int i0 = 0; i0 < len; i0 += 8) {
+        double v[10];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) mine[k] += __popc(__ballot_sync(0xffffffffu, e.hit[k]));
-      }
-      if (lane == 0)
-        for (int k = 0; k < 4; ++k) warp_count[warp][k] = mine[k];
-      __syncthreads();
-      if (tid < 4) {
-        int run = 0;
-        for (int w = 0; w < kFftThreads / 32; ++w) {
-          warp_base[w][tid] = run;
-          run += warp_count[w][tid];
-        }
-        block_total[tid] = run;
-      }
-      __syncthreads();
-      int at[4], added[4];
+        for (int u = 0; u < 10; ++u) v[u] = X(i0 + u);
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        at[k] = count[k] + warp_base[warp][k];
-        added[k] = block_total[k];
-      }
-      for (int q0 = q_begin; q0 < q_end; q0 += 32) {
-        const int q = q0 + lane;
-        const Events e = detect(xs, 2 * H + q, o + q, q < q_end, q < peak_end);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const unsigned m = __ballot_sync(0xffffffffu, e.hit[k]);
-          if (e.hit[k]) ev[k][at[k] + __popc(m & below)] = e.fine[k];
-          at[k] += __popc(m);
+        for (int u = 0; u < 8; ++u) {
+          const int q = q_lo + i0 + u;
+          if (i0 + u >= len) break;
+          const double f0 = v[u], f1 = v[u + 1], f2 = v[u + 2];
+          const double a0 = -f0, a1 = -f1, a2 = -f2;
+          const double d0 = a0 - a1, d1 = a1 - a2;
+          mine += (0.0 < f0 && f1 <= 0.0) ? 1ull : 0ull;
+          mine += (0.0 < a0 && a1 <= 0.0) ? (1ull << 16) : 0ull;
+          if (q < peak_end) {
+            mine += (0.0 < d0 && d1 <= 0.0) ? (1ull << 32) : 0ull;
+            mine += (0.0 < -d0 && -d1 <= 0.0) ? (1ull << 48) : 0ull;
+          }
         }
       }
+      unsigned long long total;
+      const unsigned long long before = block_scan_packed(mine, scan_scratch, total);
+      int at[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) count[k] += added[k];
+      for (int k = 0; k < 4; ++k) at[k] = count[k] + static_cast<int>((before >> (16 * k)) & 0xffff);
+      for (int i0 = 0; i0 < len; i0 += 8) {
+        double v[10];
+#pragma unroll
+        for (int u = 0; u < 10; ++u) v[u] = X(i0 + u);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int q = q_lo + i0 + u;
+          if (i0 + u >= len) break;
+          const double f0 = v[u], f1 = v[u + 1], f2 = v[u + 2];
+          const int64_t e = o + q + 1;
+          const double a0 = -f0, a1 = -f1, a2 = -f2;
+          const double d0 = a0 - a1, d1 = a1 - a2;
+          if (0.0 < f0 && f1 <= 0.0) ev[0][at[0]++] = fine_edge(e, f0, f1);
+          if (0.0 < a0 && a1 <= 0.0) ev[1][at[1]++] = fine_edge(e, a0, a1);
+          if (q < peak_end) {
+            if (0.0 < d0 && d1 <= 0.0) ev[2][at[2]++] = fine_edge(e, d0, d1);
+            const double e0 = -d0, e1 = -d1;
+            if (0.0 < e0 && e1 <= 0.0) ev[3][at[3]++] = fine_edge(e, e0, e1);
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) count[k] += static_cast<int>((total >> (16 * k)) & 0xffff);
     }
     __syncthreads();
     const int64_t f_begin = B.frame_off[c];

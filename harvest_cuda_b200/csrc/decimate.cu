@@ -120,6 +120,16 @@ __global__ void decimate_segment_run(DecimateView v, const double* __restrict__ 
   }
 }
 
+// Sets *flag if any sample is not finite (the reference rejects such input,
+// src/bindings.cpp:36-38); checked by the host before results are copied.
+__global__ void flag_nonfinite(const double* __restrict__ x, int64_t total, int* __restrict__ flag) {
+  bool bad = false;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x)
+    bad |= !isfinite(x[i]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) *flag = 1;
+}
+
 // Ratio 1: the waveform is used as is (harvest.cpp:45-48).
 __global__ void copy_clips(const double* __restrict__ x, int64_t total, double* __restrict__ y) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -198,6 +208,11 @@ cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, d
   decimate_segment_states<1><<<grid, threads, 0, stream>>>(v, x, u, segments, states);
   decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
   decimate_segment_run<1><<<grid, threads, 0, stream>>>(v, x, u, segments, states, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_check_finite(const double* x, int64_t total, int* flag, int sms, cudaStream_t stream) {
+  flag_nonfinite<<<sms * 4, 256, 0, stream>>>(x, total, flag);
   return cudaGetLastError();
 }
 

@@ -25,7 +25,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/harvest_b200.h"
+#include "harvest_b200.h"
 #include "hv_stages.cuh"
 
 namespace hv {
@@ -288,7 +288,7 @@ struct Plan {
   void* meta = nullptr;
   size_t arena_bytes = 0;
   struct Layout {
-    size_t x, u, states, y, bins, queue, slots, spectra, raw, cand, count, jobs, classes, refined, scores, pruned,
+    size_t x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores, pruned,
         pruned_scores, best, smoothed, scratch, f0, times;
   } at{};
   int bank_ctas = 0;
@@ -330,6 +330,7 @@ struct Workspace {
   size_t arena_size = 0;
   int sms = 0;
   double2* twiddles = nullptr;  // e^{-2 pi i t / 8192}, t < 8192
+  int* host_flag = nullptr;      // pinned word for the non-finite-sample flag
   std::map<Settings, std::shared_ptr<const BankTables>> banks;
   std::list<std::unique_ptr<Plan>> plans;  // most recent first
 
@@ -340,6 +341,7 @@ struct Workspace {
     check(cudaEventCreateWithFlags(&last, cudaEventDisableTiming), "cudaEventCreate");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
     check(cudaMalloc(&twiddles, sizeof(double2) * fft_bank_block_length()), "cudaMalloc(twiddles)");
+    check(cudaHostAlloc(reinterpret_cast<void**>(&host_flag), sizeof(int), cudaHostAllocDefault), "cudaHostAlloc");
     check(launch_twiddles(twiddles, stream), "twiddles");
     check(cudaStreamSynchronize(stream), "twiddles");
   }
@@ -351,6 +353,7 @@ struct Workspace {
       plans.clear();
       if (arena) cudaFree(arena);
       if (twiddles) cudaFree(twiddles);
+      if (host_flag) cudaFreeHost(host_flag);
       for (auto& e : marks) if (e) cudaEventDestroy(e);
       if (last) cudaEventDestroy(last);
       if (stream) cudaStreamDestroy(stream);
@@ -535,6 +538,7 @@ struct Workspace {
     p->at.y = take(8 * p->y_off[B]);
     p->at.bins = take(8 * 3 * B);
     p->at.queue = take(16);
+    p->at.flag = take(16);
     p->at.slots = take(8 * 4 * p->slot_capacity * p->bank_ctas);
     p->at.spectra = take(sizeof(double2) * (block / 2 + 1) * p->total_blocks);
     p->at.raw = take(8 * size_t(p->bands) * F);
@@ -570,6 +574,8 @@ struct Workspace {
     double* x = ptr<double>(p.at.x);
     double* y = ptr<double>(p.at.y);
     mark(0);
+    check(cudaMemsetAsync(ptr<int>(p.at.flag), 0, 16, s), "memset");
+    check(launch_check_finite(x, p.x_off[B], ptr<int>(p.at.flag), sms, s), "check_finite");
     if (p.ratio > 1) {
       DecimateView dv{};
       dv.clips = B; dv.ratio = p.ratio; dv.lag = p.lag; dv.seg_len = kSegment;
@@ -591,7 +597,8 @@ struct Workspace {
     kv.max_pad_taps = p.bank->max_pad_taps; kv.total_frames = F; kv.slot_capacity = p.slot_capacity;
     check(cudaMemsetAsync(ptr<int>(p.at.queue), 0, 16, s), "memset");
     if (p.use_fft) {
-      FftBankGeometry geo{p.bank->max_half, p.fft_valid, p.total_blocks, p.d_blk_off};
+      const int run = 2 * ((p.fft_valid + 2 + 2 * 256 - 1) / (2 * 256));
+      FftBankGeometry geo{p.bank->max_half, p.fft_valid, run, p.total_blocks, p.d_blk_off};
       check(launch_fft_bank(kv, geo, y, ptr<double>(p.at.bins), twiddles, p.filters, ptr<double2>(p.at.spectra),
                             ptr<int>(p.at.queue), ptr<double>(p.at.slots), p.bank_ctas, ptr<double>(p.at.raw), s),
             "band_bank_fft");
@@ -732,6 +739,15 @@ void run_host(const double* x, const int64_t* offsets, int clips, const Settings
   check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyHostToDevice, ws.stream),
         "cudaMemcpy(x)");
   ws.run(p, ws.stream, use_graph, record);
+  // Samples are checked for finiteness on the device; nothing is copied back
+  // for input the reference would have rejected.
+  check(cudaMemcpyAsync(ws.host_flag, ws.ptr<int>(p.at.flag), sizeof(int), cudaMemcpyDeviceToHost, ws.stream),
+        "cudaMemcpy(flag)");
+  check(cudaStreamSynchronize(ws.stream), "harvest");
+  if (*ws.host_flag) {
+    check(cudaEventRecord(ws.last, ws.stream), "cudaEventRecord");
+    throw InvalidArgument("x must contain only finite samples");
+  }
   check(cudaMemcpyAsync(f0, ws.ptr<double>(p.at.f0), 8 * total_out, cudaMemcpyDeviceToHost, ws.stream),
         "cudaMemcpy(f0)");
   if (times)
@@ -781,7 +797,6 @@ int hv_harvest(const double* x, int64_t n, int fs, double f0_floor, double f0_ce
   return guarded([&] {
     validate_settings(n, fs, f0_floor, f0_ceil, frame_period);
     if (!x || !f0 || !times) throw InvalidArgument("null buffer");
-    validate_samples(x, n);
     if (out_len != samples_for(fs, n, frame_period)) throw InvalidArgument("output length mismatch");
     int64_t offsets[2] = {0, n};
     run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, false);
@@ -793,7 +808,6 @@ int hv_profile(const double* x, int64_t n, int fs, double f0_floor, double f0_ce
   return guarded([&] {
     validate_settings(n, fs, f0_floor, f0_ceil, frame_period);
     if (!x || !f0 || !times || !stage_ms) throw InvalidArgument("null buffer");
-    validate_samples(x, n);
     if (out_len != samples_for(fs, n, frame_period)) throw InvalidArgument("output length mismatch");
     int64_t offsets[2] = {0, n};
     run_host(x, offsets, 1, Settings{fs, f0_floor, f0_ceil, frame_period}, device, f0, times, false, true);
@@ -826,7 +840,6 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
     const bool record = (flags & HV_RECORD_STAGES) != 0;
     const bool use_graph = !(flags & HV_NO_GRAPH) && !record;
     if (!(flags & HV_DEVICE_POINTERS)) {
-      validate_samples(x + offsets[0], offsets[clips] - offsets[0]);
       run_host(x, offsets, clips, s, device, f0, times, use_graph, record);
       return;
     }

@@ -106,6 +106,51 @@ __device__ __forceinline__ void stockham_pass(double2* buf, const double2* __res
   __syncthreads();
 }
 
+// Exact quotient q / d for 0 <= q < 2^24 without an integer division: a
+// float reciprocal estimate corrected by one step either way.
+struct RunDivider {
+  int d;
+  float inv;
+  __device__ __forceinline__ int operator()(int q) const {
+    int r = static_cast<int>(static_cast<float>(q) * inv);
+    if (r * d > q) --r;
+    else if ((r + 1) * d <= q) ++r;
+    return r;
+  }
+};
+
+// Last pass of an inverse transform whose result is read as 8192 real
+// samples x[2m] = Re z[m], x[2m+1] = Im z[m]: instead of storing z in natural
+// order it stores samples p >= first into lin[(p - first) + (p - first) / run],
+// one pad slot per `run` samples, the layout the event scan reads.
+__device__ __forceinline__ void inverse_last_pass_to_runs(double2* buf, const double2* __restrict__ tw,
+                                                          int first, RunDivider run) {
+  const int j = threadIdx.x;
+  const int ls = 256;
+  const int k = j & (ls - 1);
+  double2 x[16];
+#pragma unroll
+  for (int m = 0; m < 16; ++m) x[m] = buf[fpad(j + m * (kFftN / 16))];
+  const double2 w = twiddle<+1>(tw, k * (2 * kFftN / (16 * ls)));
+  double2 wm = w;
+#pragma unroll
+  for (int m = 1; m < 16; ++m) {
+    x[m] = cmul(x[m], wm);
+    wm = cmul(wm, w);
+  }
+  dft16<+1>(x);
+  __syncthreads();
+  double* lin = reinterpret_cast<double*>(buf);
+  const int out0 = (j - k) * 16 + k;
+#pragma unroll
+  for (int m = 0; m < 16; ++m) {
+    const int p = 2 * (out0 + m * ls) - first;
+    if (p >= 0) lin[p + run(p)] = x[m].x;
+    if (p + 1 >= 0) lin[p + 1 + run(p + 1)] = x[m].y;
+  }
+  __syncthreads();
+}
+
 // Full transform of buf (natural order in and out). Callers synchronise
 // before the first pass; the last pass ends with a barrier.
 template <int kSign>

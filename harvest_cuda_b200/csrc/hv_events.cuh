@@ -57,6 +57,28 @@ __device__ inline void final_bin_terms(const double* __restrict__ taps, int half
   c1i = (qi - pi) * scale;
 }
 
+// Exclusive scan over the block of four 16-bit counters packed in 64 bits;
+// `scratch` holds blockDim.x / 32 words. Every thread receives the total.
+__device__ inline unsigned long long block_scan_packed(unsigned long long v, unsigned long long* scratch,
+                                                       unsigned long long& total) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  unsigned long long inc = v;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long n = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += n;
+  }
+  __syncthreads();
+  if (lane == 31) scratch[warp] = inc;
+  __syncthreads();
+  unsigned long long before = 0, all = 0;
+  for (int w = 0; w < warps; ++w) {
+    if (w < warp) before += scratch[w];
+    all += scratch[w];
+  }
+  total = all;
+  return before + inc - v;
+}
+
 // Sub-sample position of a negative-going crossing between s0 > 0 and
 // s1 <= 0 at integer edge e (harvest.cpp:184-186).
 __device__ __forceinline__ double fine_edge(int64_t e, double s0, double s1) {
@@ -141,13 +163,13 @@ __device__ inline void band_contour_staged(const BatchView& B, double* const ev[
   for (int g0 = 0; g0 < chunks; g0 += nt) {
     const int group = imin(nt, chunks - g0);
     __syncthreads();
-    if (tid < group) {
-      const int first = (g0 + tid) * nt;
-      const int last = imin(first + nt, frames) - 1;
-      for (int k = 0; k < 4; ++k) {
-        bounds[(2 * k) * nt + tid] = segment_at(ev[k], count[k], fs, first * 1 / 1000.0);
-        bounds[(2 * k + 1) * nt + tid] = segment_at(ev[k], count[k], fs, last * 1 / 1000.0);
-      }
+    // 8 searches per chunk (first and last frame, four tracks), one per
+    // thread, so their dependent loads overlap instead of queueing.
+    for (int w = tid; w < 8 * group; w += nt) {
+      const int ci = w >> 3, which = w & 7, k = which >> 1;
+      const int first = (g0 + ci) * nt;
+      const int frame = (which & 1) ? imin(first + nt, frames) - 1 : first;
+      bounds[which * nt + ci] = segment_at(ev[k], count[k], fs, frame * 1 / 1000.0);
     }
     __syncthreads();
     for (int ci = 0; ci < group; ++ci) {
@@ -179,33 +201,54 @@ __device__ inline void band_contour_staged(const BatchView& B, double* const ev[
       if (f >= frames) continue;
       const double t = f * 1 / 1000.0;
       double track[4];
-      for (int k = 0; k < 4; ++k) {
-        double x0, x1, y0, y1;
-        if (staged) {
+      if (staged) {
+        // The four searches are independent; unrolled they overlap.
+        int a[4], b[4];
+        const double* loc[4];
+        const double* val[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
           const int n_int = hi[k] - lo[k] + 2;
-          const double* loc = stage + base[k] - (lo[k] - 1);   // loc[j], j in [lo-1, hi]
-          const double* val = loc + n_int;
-          // seg = lo + #{j in [lo, hi) : loc[j] <= t}
-          int a = lo[k], b = hi[k];
-          while (a < b) {
-            const int mid = (a + b) >> 1;
-            if (loc[mid] <= t) a = mid + 1; else b = mid;
+          loc[k] = stage + base[k] - (lo[k] - 1);   // loc[j], j in [lo-1, hi]
+          val[k] = loc[k] + n_int;
+          a[k] = lo[k];
+          b[k] = hi[k];
+        }
+        // seg = lo + #{j in [lo, hi) : loc[j] <= t}
+        bool more = true;
+        while (more) {
+          more = false;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            if (a[k] < b[k]) {
+              const int mid = (a[k] + b[k]) >> 1;
+              if (loc[k][mid] <= t) a[k] = mid + 1; else b[k] = mid;
+              more |= a[k] < b[k];
+            }
           }
-          x0 = loc[a - 1]; x1 = loc[a]; y0 = val[a - 1]; y1 = val[a];
-        } else {
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double x0 = loc[k][a[k] - 1], x1 = loc[k][a[k]];
+          const double y0 = val[k][a[k] - 1], y1 = val[k][a[k]];
+          const double s = (t - x0) / (x1 - x0);
+          track[k] = y0 + s * (y1 - y0);
+        }
+      } else {
+        for (int k = 0; k < 4; ++k) {
           const double* e = ev[k];
           int a = lo[k], b = hi[k];
           while (a < b) {
             const int mid = (a + b) >> 1;
             if ((e[mid] + e[mid + 1]) / 2.0 / fs <= t) a = mid + 1; else b = mid;
           }
-          x0 = (e[a - 1] + e[a]) / 2.0 / fs;
-          x1 = (e[a] + e[a + 1]) / 2.0 / fs;
-          y0 = fs / (e[a] - e[a - 1]);
-          y1 = fs / (e[a + 1] - e[a]);
+          const double x0 = (e[a - 1] + e[a]) / 2.0 / fs;
+          const double x1 = (e[a] + e[a + 1]) / 2.0 / fs;
+          const double y0 = fs / (e[a] - e[a - 1]);
+          const double y1 = fs / (e[a + 1] - e[a]);
+          const double s = (t - x0) / (x1 - x0);
+          track[k] = y0 + s * (y1 - y0);
         }
-        const double s = (t - x0) / (x1 - x0);
-        track[k] = y0 + s * (y1 - y0);
       }
       double val = (track[0] + track[1] + track[2] + track[3]) / 4.0;
       if (val > upper || val < lower || val > B.f0_ceil || val < B.f0_floor) val = 0.0;

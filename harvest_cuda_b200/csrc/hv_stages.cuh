@@ -49,6 +49,7 @@ struct ContourView {
 cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, double* states,
                             int64_t segments, double* y, cudaStream_t stream);
 cudaError_t launch_copy(const double* x, int64_t total, double* y, cudaStream_t stream);
+cudaError_t launch_check_finite(const double* x, int64_t total, int* flag, int sms, cudaStream_t stream);
 cudaError_t launch_remove_mean(const BatchView& v, double* y, double* bins, cudaStream_t stream);
 
 size_t band_bank_smem_bytes(int max_pad_taps);
@@ -64,6 +65,7 @@ cudaError_t launch_band_bank(const BankView& v, const double* y, const double* e
 struct FftBankGeometry {
   int max_half;
   int valid;
+  int run;                 // event-scan positions per thread: even, run * 256 >= valid + 2
   int64_t total_blocks;
   const int64_t* blk_off;  // [clips + 1] block offsets
 };

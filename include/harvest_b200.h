@@ -70,7 +70,10 @@ HV_API int hv_harvest(const double* x, int64_t n, int fs, double f0_floor, doubl
  * hv_output_length(offsets[c+1] - offsets[c], fs, frame_period). With
  * HV_DEVICE_POINTERS, x/f0/times are device memory and the work is ordered
  * on `stream` (a cudaStream_t, NULL for the engine's own stream); the call
- * returns once the work is enqueued. Without it, the call is synchronous.
+ * returns once the work is enqueued, and non-finite samples cannot be
+ * reported (they yield unspecified F0 values, never a fault). Without it,
+ * the call is synchronous and rejects non-finite samples with
+ * HV_INVALID_ARGUMENT, checked on the device before any output is copied.
  * No counterpart in the reference, which processes one clip per call. */
 HV_API int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
                      double f0_floor, double f0_ceil, double frame_period, int device,
