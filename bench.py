@@ -415,6 +415,17 @@ def stage_models(wl):
     return models
 
 
+def ncu_traffic(stage, wl):
+    """DRAM bytes per launch of `stage` for this workload, scaled by audio
+    seconds from the ncu capture summarised in profiles/ (None if absent)."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        per = json.load(f)["bytes_per_audio_second"].get(stage)
+    return None if per is None else per * float(sum(wl["lengths"])) / wl["fs"]
+
+
 def summarize(args, wl, value, ms, stages, e2e, clocks, device, world):
     hbm, hbm_src = load_peaks()
     models = stage_models(wl)
@@ -422,7 +433,7 @@ def summarize(args, wl, value, ms, stages, e2e, clocks, device, world):
     nbytes, flops = models[dominant]
     dur = stages[dominant] / 1000.0
     roof = {"bound": "hbm", "kernel": dominant, "achieved": nbytes / dur / 1e9, "peak": hbm,
-            "unit": "GB/s", "frac": nbytes / dur / 1e9 / hbm, "traffic": None,
+            "unit": "GB/s", "frac": nbytes / dur / 1e9 / hbm, "traffic": ncu_traffic(dominant, wl),
             "peak_source": hbm_src, "algorithmic_bytes": nbytes, "launch_ms": stages[dominant]}
     peak64 = fp64_peak(device)
     if flops is not None and peak64:
