@@ -39,6 +39,8 @@ SIGNATURES = {
                               ct.c_int, _D, _D, ct.c_int64, _D]),
     "hv_harvest_stages": (ct.c_int, [_D, ct.c_int64, ct.c_int, ct.c_double, ct.c_double, ct.c_int,
                                      _D, _D, ct.POINTER(ct.c_int), _D, _D, _D, _D, _D, _D, _D]),
+    "hv_decimate_noalloc": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, ct.c_int, ct.c_void_p,
+                                       ct.c_void_p]),
     "hv_clear_cache": (ct.c_int, []),
 }
 

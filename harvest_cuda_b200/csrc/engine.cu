@@ -758,6 +758,45 @@ void run_host(const double* x, const int64_t* offsets, int clips, const Settings
   if (record) collect_stage_ms(ws);
 }
 
+// ---------------------------------------------- allocation-free decimation --
+// Scratch of hv_decimate_noalloc: a fixed array in the library's device
+// image, present on every GPU that loads the library for the life of the
+// process. It holds the forward low-pass pass (n + 2 lag + 18 doubles), the
+// segment states (3 per 256 samples), the clip offsets and two spare words.
+constexpr int64_t kNoAllocMaxSamples = int64_t(1) << 20;
+constexpr int64_t kNoAllocPadded = kNoAllocMaxSamples + 2 * 151 + 18;   // lag <= 151
+constexpr int64_t kNoAllocSegments = (kNoAllocPadded + kSegment - 1) / kSegment;
+constexpr int64_t kNoAllocMeta = 16;                                      // offsets, nfft, bins
+constexpr int64_t kNoAllocDoubles = kNoAllocPadded + 3 * kNoAllocSegments + kNoAllocMeta;
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+// Writes the one-clip offset tables into the scratch (no host copies).
+__global__ void noalloc_tables(int64_t* meta, int64_t n, int64_t y_len, int64_t padded, int64_t segments,
+                               int nfft) {
+  meta[0] = 0; meta[1] = n;          // x_off
+  meta[2] = 0; meta[3] = y_len;      // y_off
+  meta[4] = 0; meta[5] = padded;     // t_off
+  meta[6] = 0; meta[7] = segments;   // seg_off
+  reinterpret_cast<int*>(meta + 8)[0] = nfft;
+}
+
+// Device address of the scratch per device, resolved once with that device's
+// primary context current.
+struct NoAllocDevice {
+  std::once_flag once;
+  std::unique_ptr<PrimaryContext> ctx;
+  double* scratch = nullptr;
+  cudaError_t status = cudaSuccess;
+};
+NoAllocDevice& noalloc_device(int device) {
+  static std::mutex mutex;
+  static std::map<int, std::unique_ptr<NoAllocDevice>> devices;
+  std::lock_guard<std::mutex> lock(mutex);
+  auto& slot = devices[device];
+  if (!slot) slot = std::make_unique<NoAllocDevice>();
+  return *slot;
+}
+
 }  // namespace
 }  // namespace hv
 
@@ -903,6 +942,65 @@ int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor, doubl
     out(smoothed, p.at.smoothed, 8 * F);
     check(cudaEventRecord(ws.last, ws.stream), "cudaEventRecord");
     check(cudaStreamSynchronize(ws.stream), "harvest_stages");
+  });
+}
+
+int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* y, void* stream) {
+  return guarded([&] {
+    if (fs < 8000 || fs > 192000) throw InvalidArgument("fs must be between 8000 and 192000 Hz");
+    const int ratio = ratio_for(fs);
+    if (n < int64_t(2) * ratio)
+      throw InvalidArgument("x is too short: require at least two samples after internal decimation");
+    if (n > kNoAllocMaxSamples)
+      throw InvalidArgument("hv_decimate_noalloc accepts at most " + std::to_string(kNoAllocMaxSamples) +
+                            " samples per call (its device scratch is fixed); use hv_harvest_batch for longer input");
+    if (!x || !y) throw InvalidArgument("null buffer");
+    check_device(device);
+    NoAllocDevice& dev = noalloc_device(device);
+    std::call_once(dev.once, [&] {
+      dev.ctx = std::make_unique<PrimaryContext>(device);
+      ContextGuard g(dev.ctx->get());
+      void* address = nullptr;
+      dev.status = cudaGetSymbolAddress(&address, g_noalloc_scratch);
+      dev.scratch = static_cast<double*>(address);
+    });
+    check(dev.status, "cudaGetSymbolAddress(scratch)");
+    if (!dev.scratch) throw RuntimeFailure("device scratch unavailable");
+    ContextGuard guard(dev.ctx->get());
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int64_t y_len = (n + ratio - 1) / ratio;
+    const int lag = static_cast<int>(std::ceil(140.0 / ratio) * ratio);
+    const int64_t padded = ratio > 1 ? n + 2 * lag + 18 : 0;
+    const int64_t segments = ratio > 1 ? (padded + kSegment - 1) / kSegment : 0;
+    double* u = dev.scratch;
+    double* states = u + kNoAllocPadded;
+    int64_t* meta = reinterpret_cast<int64_t*>(states + 3 * kNoAllocSegments);
+    double* bins = reinterpret_cast<double*>(meta + 10);
+    noalloc_tables<<<1, 1, 0, s>>>(meta, n, y_len, padded, segments, static_cast<int>(2 * y_len));
+    check(cudaGetLastError(), "noalloc_tables");
+    BatchView bv{};
+    bv.clips = 1; bv.ratio = ratio; bv.fs_r = double(fs) / ratio;
+    bv.x_off = meta; bv.y_off = meta + 2; bv.frame_off = meta + 2;
+    bv.nfft = reinterpret_cast<const int*>(meta + 8);
+    if (ratio > 1) {
+      DecimateView dv{};
+      dv.clips = 1; dv.ratio = ratio; dv.lag = lag; dv.seg_len = kSegment;
+      std::memcpy(dv.a, kLowA[ratio], sizeof dv.a);
+      std::memcpy(dv.b, kLowB[ratio], sizeof dv.b);
+      const double* a = kLowA[ratio];
+      double A[9] = {a[0], a[1], a[2], 1, 0, 0, 0, 1, 0};
+      double R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+      for (int e = kSegment; e; e >>= 1) {
+        if (e & 1) mat3_mul(R, A, R);
+        mat3_mul(A, A, A);
+      }
+      std::memcpy(dv.trans, R, sizeof R);
+      dv.x_off = meta; dv.y_off = meta + 2; dv.t_off = meta + 4; dv.seg_off = meta + 6;
+      check(launch_decimate(dv, x, u, states, segments, y, s), "decimate");
+    } else {
+      check(launch_copy(x, n, y, s), "copy");
+    }
+    check(launch_remove_mean(bv, y, bins, s), "remove_mean");
   });
 }
 

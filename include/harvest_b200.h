@@ -103,6 +103,32 @@ HV_API int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor
                              double* refined, double* scores, double* pruned,
                              double* pruned_scores, double* best, double* smoothed);
 
+/* Allocation-free decimation: the decimation and DC-removal stage of
+ * hv_harvest on one clip, for callers that cannot allocate device memory
+ * at the point of the call: real-time audio callbacks that must not block
+ * inside the driver's allocator, processes whose GPU memory is wholly held
+ * by a caching allocator or a fixed budget, and deployments that forbid
+ * device allocation after start-up. It has no counterpart in the
+ * reference, whose decimation always allocates a workspace.
+ *
+ * x (n samples) and y (ceil(n / r) samples, r = clamp(round(fs / 8000),
+ * 1, 12)) are device pointers on `device`; the work is enqueued on `stream`
+ * (a cudaStream_t of that device's primary context, NULL for its default
+ * stream) and the call returns without waiting. y receives exactly what
+ * hv_harvest_stages returns as y.
+ *
+ * The scratch is one fixed array in the library's device image (about
+ * 8.5 MB, held on every GPU that loads the library until the process
+ * exits), so n may not exceed 1048576 samples; longer input is rejected
+ * with HV_INVALID_ARGUMENT. No cudaMalloc, cudaFree or other allocating
+ * routine is called. The first call on a device looks up the array's
+ * device address (cudaGetSymbolAddress) and retains the primary context;
+ * make that first call before any stream capture. Every call on a device
+ * shares the array and leaves its contents behind: each call writes every
+ * scratch word it reads, so nothing needs clearing, but calls whose work
+ * overlaps on the GPU (different streams without ordering) race on it. */
+HV_API int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* y, void* stream);
+
 /* Releases cached device and host working memory on every device.
  * Workspaces in use finish their call first (reference bindings.cpp:60-65,
  * src/workspace_cache.h:61-70). */
