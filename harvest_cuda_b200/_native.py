@@ -41,6 +41,12 @@ SIGNATURES = {
                                      _D, _D, ct.POINTER(ct.c_int), _D, _D, _D, _D, _D, _D, _D]),
     "hv_decimate_noalloc": (ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, ct.c_int, ct.c_void_p,
                                        ct.c_void_p]),
+    "hv_harvest_grad_forward": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                           ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                           ct.c_void_p]),
+    "hv_harvest_grad_backward": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                            ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                            ct.c_void_p]),
     "hv_clear_cache": (ct.c_int, []),
 }
 

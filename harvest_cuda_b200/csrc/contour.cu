@@ -337,6 +337,144 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
   }
 }
 
+// Tape of the F0 gradient, written after contour_clips while its scratch is
+// live: per frame the step-3 value and the initial F0 of the candidate it
+// copies. Every nonzero step-3 value is a copy of a pruned candidate of its
+// own frame (FixStep1 keeps SearchF0Base's pick; ExtendF0 and MergeF0 copy
+// candidates), so the first column holding that value identifies it; a
+// candidate's refined F0 depends on its initial F0 only through discrete
+// choices (window length, bins), so any column holding the same value
+// reproduces the same refinement.
+__global__ void record_tape(ContourView v, const double* __restrict__ cand, int64_t total_frames,
+                            double* __restrict__ tape) {
+  const int64_t gf = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (gf >= total_frames) return;
+  const BatchView& B = v.batch;
+  const int c = owner(B.frame_off, B.clips, gf);
+  const int64_t row0 = B.frame_off[c];
+  const int F = static_cast<int>(B.frame_off[c + 1] - row0);
+  const double fixed = v.scratch[v.scratch_off[c] + 2 * F + (gf - row0)];   // s3 of contour_clips
+  double f0c = 0.0;
+  if (fixed > 0.0) {
+    const double* row = v.pruned + gf * B.capacity;
+    const int columns = 7 * v.count[c];
+    for (int col = 0; col < columns; ++col)
+      if (row[col] == fixed) { f0c = overlapped_candidate(B, cand, v.count, gf, col); break; }
+  }
+  tape[2 * gf] = fixed;
+  tape[2 * gf + 1] = f0c;
+}
+
+// Transpose of the resampling, SmoothF0Contour and FixStep4 for the F0
+// gradient, with the voicing held fixed; one warp per clip. From dL/df0 at
+// the output frames it forms dL/d(step-3 value) per 1 ms frame:
+//   * resampling: an output frame's gradient goes to the frame it copies;
+//   * smoothing: each voiced section is smoothed by a linear map (held
+//     padding, Butterworth pass, reversal, pass, reversal); its transpose is
+//     the same two passes over the section's gradient, zero outside it,
+//     followed by summing the held regions into the section's end frames.
+//     The free response beyond kTransient samples past either end
+//     (below 0.88^1024 of the peak) is dropped;
+//   * FixStep4: a frame filled cnt frames into a gap of d frames between
+//     sections ending at a and starting at b depends on the step-3 values
+//     at a and b with weights 1 - cnt / (d + 1) and cnt / (d + 1).
+__global__ void __launch_bounds__(32) contour_adjoint(GradView v) {
+  const int c = blockIdx.x;
+  const int lane = threadIdx.x;
+  const BatchView& B = v.batch;
+  const int64_t row0 = B.frame_off[c];
+  const int F = static_cast<int>(B.frame_off[c + 1] - row0);
+  double* s3 = v.scratch + v.scratch_off[c];
+  double* s4 = s3 + F;
+  double* g_sm = s4 + F;
+  double* g_s4 = g_sm + F;
+  double* g_s3 = g_s4 + F;
+  double* weight = g_s3 + F;        // cnt / (d + 1) of a filled frame, -1 elsewhere
+  double* body = weight + F;        // a section's gradient after the first pass
+  double* tails = body + F;         // 32 x kTransient
+  int* bl = reinterpret_cast<int*>(tails + 32 * kTransient);   // up to F + 602 ints
+  for (int i = lane; i < F; i += 32) {
+    s3[i] = s4[i] = v.tape[2 * (row0 + i)];
+    g_sm[i] = g_s4[i] = g_s3[i] = 0.0;
+    weight[i] = -1.0;
+  }
+  __syncwarp();
+  const int64_t o0 = v.out_off[c];
+  const int out_len = static_cast<int>(v.out_off[c + 1] - o0);
+  for (int i = lane; i < out_len; i += 32) {
+    const double t = i * v.period / 1000.0;
+    atomicAdd(g_sm + imin(F - 1, matlab_round(t * 1000.0)), v.grad_f0[o0 + i]);
+  }
+  // FixStep4's fills, as contour_clips computes them.
+  int nb = warp_boundary_list([&](int i) { return s3[i]; }, F, bl);
+  for (int i = lane; i < nb / 2 - 1; i += 32) {
+    const int a = bl[2 * i + 1], b = bl[2 * (i + 1)];
+    const int distance = b - a - 1;
+    if (distance >= 9) continue;
+    const double v0 = s3[a] + 1;
+    const double v1 = s3[b] - 1;
+    const double slope = (v1 - v0) / (distance + 1.0);
+    int cnt = 1;
+    for (int j = a + 1; j <= b - 1; ++j) {
+      weight[j] = (j - a) / (distance + 1.0);
+      s4[j] = v0 + slope * cnt++;
+    }
+  }
+  __syncwarp();
+  // Smoothing, one voiced section of the padded contour per lane.
+  const int lag = 300;
+  const int64_t len = F + 2 * lag;
+  auto padded = [&](int j) -> double { return (j >= lag && j < lag + F) ? s4[j - lag] : 0.0; };
+  const int nbs = warp_boundary_list(padded, static_cast<int>(len), bl);
+  for (int sec = lane; sec < nbs / 2; sec += 32) {
+    const int st = bl[2 * sec], ed = bl[2 * sec + 1];
+    Butter fw;
+    for (int j = st; j <= ed; ++j) body[j - lag] = fw.step(g_sm[j - lag]);
+    double* tail = tails + lane * kTransient;
+    const int64_t trailing = len - 1 - ed < kTransient ? len - 1 - ed : kTransient;
+    for (int64_t k = 0; k < trailing; ++k) tail[k] = fw.step(0.0);
+    Butter bw;
+    double held = 0.0;
+    for (int64_t k = trailing - 1; k >= 0; --k) held += bw.step(tail[k]);
+    for (int j = ed; j >= st; --j) g_s4[j - lag] = bw.step(body[j - lag]);
+    g_s4[ed - lag] += held;
+    held = 0.0;
+    const int leading = st < kTransient ? st : kTransient;
+    for (int k = 0; k < leading; ++k) held += bw.step(0.0);
+    g_s4[st - lag] += held;
+  }
+  __syncwarp();
+  // FixStep4: unfilled frames pass through; each gap then adds to its left
+  // end, and (after a barrier, since one frame can end one gap and start the
+  // next) to its right end.
+  for (int i = lane; i < F; i += 32)
+    if (weight[i] < 0.0) g_s3[i] = g_s4[i];
+  __syncwarp();
+  nb = warp_boundary_list([&](int i) { return s3[i]; }, F, bl);
+  for (int side = 0; side < 2; ++side) {
+    for (int i = lane; i < nb / 2 - 1; i += 32) {
+      const int a = bl[2 * i + 1], b = bl[2 * (i + 1)];
+      if (b - a - 1 >= 9) continue;
+      double acc = 0.0;
+      for (int j = a + 1; j <= b - 1; ++j) acc += (side ? weight[j] : 1.0 - weight[j]) * g_s4[j];
+      g_s3[side ? b : a] += acc;
+    }
+    __syncwarp();
+  }
+  for (int i = lane; i < F; i += 32) v.grad_fixed[row0 + i] = s3[i] > 0.0 ? g_s3[i] : 0.0;
+}
+
+cudaError_t launch_tape(const ContourView& v, const double* cand, int64_t total_frames, double* tape,
+                        cudaStream_t stream) {
+  record_tape<<<static_cast<unsigned>((total_frames + 255) / 256), 256, 0, stream>>>(v, cand, total_frames, tape);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream) {
+  contour_adjoint<<<v.batch.clips, 32, 0, stream>>>(v);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_contour(const ContourView& v, cudaStream_t stream) {
   contour_clips<<<v.batch.clips, 32, 0, stream>>>(v);
   return cudaGetLastError();

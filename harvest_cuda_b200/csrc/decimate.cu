@@ -120,6 +120,116 @@ __global__ void decimate_segment_run(DecimateView v, const double* __restrict__ 
   }
 }
 
+// Adjoint of the decimation for the F0 gradient. The forward map is
+// y = S F R F P x: P edge-holds the clip, F is the causal low-pass with
+// zero initial state, R reverses, S keeps every r-th sample. With
+// F^T = R F R its transpose is P^T R F R F S^T: the kept-sample gradient is
+// spread onto the padded grid, reversed and low-passed (pass 0), reversed
+// and low-passed again (pass 1), and the held regions are summed into the
+// clip's first and last samples. Both passes reuse the blocked
+// state-passing scan of the forward decimation.
+
+// Pass 0 input at padded index i: S^T dL/dy read in reverse.
+__device__ __forceinline__ double kept_gradient(const DecimateView& v, const double* gy, int c, int64_t total,
+                                                int64_t i) {
+  const int r = v.ratio;
+  const int64_t m = total - 18;
+  const int64_t nout = (m - 1) / r + 1;
+  const int64_t nbeg = r - r * nout + m;
+  const int64_t dist = (total - 9 - nbeg) - (total - 1 - i);
+  if (dist < 0 || dist % r) return 0.0;
+  const int64_t k = dist / r - v.lag / r;
+  return k >= 0 && k < v.y_off[c + 1] - v.y_off[c] ? gy[v.y_off[c] + k] : 0.0;
+}
+
+template <int kPass>
+__global__ void adjoint_segment_states(DecimateView v, const double* __restrict__ gy,
+                                       const double* __restrict__ u, int64_t segments,
+                                       double* __restrict__ states) {
+  int64_t seg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  int c; int64_t begin, end;
+  clip_of_segment(v, seg, c, begin, end);
+  int64_t total = v.t_off[c + 1] - v.t_off[c];
+  const double* uc = u + v.t_off[c];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  for (int64_t i = begin; i < end; ++i) {
+    double in = kPass == 0 ? kept_gradient(v, gy, c, total, i) : uc[total - 1 - i];
+    lowpass_step(v, in, s0, s1, s2);
+  }
+  states[3 * seg + 0] = s0;
+  states[3 * seg + 1] = s1;
+  states[3 * seg + 2] = s2;
+}
+
+// Pass 0 writes the first low-passed sequence into u. Pass 1 writes the
+// gradient of every clip sample that is not held (indices 1 .. n-2) and
+// leaves the segment's sums over the held regions in its state slots.
+template <int kPass>
+__global__ void adjoint_segment_run(DecimateView v, const double* __restrict__ gy, double* __restrict__ u,
+                                    int64_t segments, double* __restrict__ states, double* __restrict__ gx) {
+  int64_t seg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  int c; int64_t begin, end;
+  clip_of_segment(v, seg, c, begin, end);
+  int64_t total = v.t_off[c + 1] - v.t_off[c];
+  double* uc = u + v.t_off[c];
+  double s0 = states[3 * seg], s1 = states[3 * seg + 1], s2 = states[3 * seg + 2];
+  if (kPass == 0) {
+    for (int64_t i = begin; i < end; ++i) uc[i] = lowpass_step(v, kept_gradient(v, gy, c, total, i), s0, s1, s2);
+    return;
+  }
+  const int64_t n = v.x_off[c + 1] - v.x_off[c];
+  double* gxc = gx + v.x_off[c];
+  double first = 0.0, last = 0.0;
+  for (int64_t j = begin; j < end; ++j) {
+    const double out = lowpass_step(v, uc[total - 1 - j], s0, s1, s2);
+    const int64_t xi = total - 1 - j - 9 - v.lag;
+    if (xi <= 0) first += out;
+    else if (xi >= n - 1) last += out;
+    else gxc[xi] = out;
+  }
+  states[3 * seg] = first;
+  states[3 * seg + 1] = last;
+}
+
+// Sums the held-region partials of every segment, in segment order.
+__global__ void adjoint_edges(DecimateView v, const double* __restrict__ states, double* __restrict__ gx) {
+  int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= v.clips) return;
+  double first = 0.0, last = 0.0;
+  for (int64_t seg = v.seg_off[c]; seg < v.seg_off[c + 1]; ++seg) {
+    first += states[3 * seg];
+    last += states[3 * seg + 1];
+  }
+  const int64_t n = v.x_off[c + 1] - v.x_off[c];
+  gx[v.x_off[c]] = first;
+  if (n > 1) gx[v.x_off[c] + n - 1] = last;
+}
+
+// Transpose of the DC removal: g -= mean(g) per clip, with the same fixed
+// reduction tree as remove_mean_and_edge_bins.
+__global__ void remove_mean_adjoint(const BatchView v, double* __restrict__ g) {
+  __shared__ double part[32];
+  int c = blockIdx.x;
+  int64_t begin = v.y_off[c], len = v.y_off[c + 1] - begin;
+  double* gc = g + begin;
+  double acc = 0.0;
+  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) acc += gc[i];
+  for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  if (!lane) part[warp] = acc;
+  __syncthreads();
+  if (warp == 0) {
+    acc = lane < warps ? part[lane] : 0.0;
+    for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (!lane) part[0] = acc;
+  }
+  __syncthreads();
+  const double mean = part[0] / len;
+  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) gc[i] -= mean;
+}
+
 // Sets *flag if any sample is not finite (the reference rejects such input,
 // src/bindings.cpp:36-38); checked by the host before results are copied.
 __global__ void flag_nonfinite(const double* __restrict__ x, int64_t total, int* __restrict__ flag) {
@@ -224,6 +334,26 @@ cudaError_t launch_copy(const double* x, int64_t total, double* y, cudaStream_t 
 
 cudaError_t launch_remove_mean(const BatchView& v, double* y, double* bins, cudaStream_t stream) {
   remove_mean_and_edge_bins<<<v.clips, 1024, 0, stream>>>(v, y, bins);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_remove_mean_adjoint(const BatchView& v, double* grad_y, cudaStream_t stream) {
+  remove_mean_adjoint<<<v.clips, 1024, 0, stream>>>(v, grad_y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_decimate_adjoint(const DecimateView& v, const double* grad_y, double* u, double* states,
+                                    int64_t segments, double* grad_x, cudaStream_t stream) {
+  const int threads = 128;
+  unsigned grid = static_cast<unsigned>((segments + threads - 1) / threads);
+  unsigned cgrid = static_cast<unsigned>((v.clips + threads - 1) / threads);
+  adjoint_segment_states<0><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states);
+  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
+  adjoint_segment_run<0><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states, grad_x);
+  adjoint_segment_states<1><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states);
+  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
+  adjoint_segment_run<1><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states, grad_x);
+  adjoint_edges<<<cgrid, threads, 0, stream>>>(v, states, grad_x);
   return cudaGetLastError();
 }
 

@@ -289,7 +289,7 @@ struct Plan {
   size_t arena_bytes = 0;
   struct Layout {
     size_t x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores, pruned,
-        pruned_scores, best, smoothed, scratch, f0, times;
+        pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed;
   } at{};
   int bank_ctas = 0;
   // Device pointers into `meta`.
@@ -555,6 +555,8 @@ struct Workspace {
     p->at.scratch = take(8 * p->scratch_off[B]);
     p->at.f0 = take(8 * p->out_off[B]);
     p->at.times = take(8 * p->out_off[B]);
+    p->at.grad_y = take(8 * p->y_off[B]);
+    p->at.grad_fixed = take(8 * F);
     p->arena_bytes = off;
     return p;
   }
@@ -562,33 +564,59 @@ struct Workspace {
   template <class T>
   T* ptr(size_t at) const { return reinterpret_cast<T*>(static_cast<char*>(arena) + at); }
 
+  static BatchView batch_view(const Plan& p) {
+    BatchView bv{};
+    bv.clips = p.clips; bv.ratio = p.ratio; bv.bands = p.bands; bv.capacity = p.capacity;
+    bv.per_group = p.per_group; bv.fs_r = p.fs_r; bv.f0_floor = p.s.floor; bv.f0_ceil = p.s.ceil;
+    bv.x_off = p.d_x_off; bv.y_off = p.d_y_off; bv.frame_off = p.d_frame_off; bv.nfft = p.d_nfft;
+    return bv;
+  }
+
+  static DecimateView decimate_view(const Plan& p) {
+    DecimateView dv{};
+    dv.clips = p.clips; dv.ratio = p.ratio; dv.lag = p.lag; dv.seg_len = kSegment;
+    std::memcpy(dv.a, kLowA[p.ratio], sizeof dv.a);
+    std::memcpy(dv.b, kLowB[p.ratio], sizeof dv.b);
+    std::memcpy(dv.trans, p.trans, sizeof dv.trans);
+    dv.x_off = p.d_x_off; dv.y_off = p.d_y_off; dv.t_off = p.d_t_off; dv.seg_off = p.d_seg_off;
+    return dv;
+  }
+
+  ContourView contour_view(const Plan& p) const {
+    ContourView cv{};
+    cv.batch = batch_view(p);
+    cv.pruned = ptr<double>(p.at.pruned); cv.pruned_scores = ptr<double>(p.at.pruned_scores);
+    cv.best = ptr<double>(p.at.best); cv.count = ptr<int>(p.at.count);
+    cv.scratch_off = p.d_scratch_off; cv.scratch = ptr<double>(p.at.scratch);
+    cv.smoothed = ptr<double>(p.at.smoothed); cv.period = p.s.period; cv.out_off = p.d_out_off;
+    cv.f0_out = ptr<double>(p.at.f0); cv.t_out = ptr<double>(p.at.times);
+    return cv;
+  }
+
+  // Decimation (or copy) of the clips at `x` into the arena's y, then DC
+  // removal.
+  void enqueue_waveform(Plan& p, const double* x, cudaStream_t s) {
+    double* y = ptr<double>(p.at.y);
+    if (p.ratio > 1)
+      check(launch_decimate(decimate_view(p), x, ptr<double>(p.at.u), ptr<double>(p.at.states), p.total_seg, y, s),
+            "decimate");
+    else
+      check(launch_copy(x, p.x_off[p.clips], y, s), "copy");
+    check(launch_remove_mean(batch_view(p), y, ptr<double>(p.at.bins), s), "remove_mean");
+  }
+
   // Enqueues every stage on `s`. With `marks_on`, records stage events.
   void enqueue(Plan& p, cudaStream_t s, bool marks_on) {
     const int B = p.clips;
     const int64_t F = p.frame_off[B];
-    BatchView bv{};
-    bv.clips = B; bv.ratio = p.ratio; bv.bands = p.bands; bv.capacity = p.capacity;
-    bv.per_group = p.per_group; bv.fs_r = p.fs_r; bv.f0_floor = p.s.floor; bv.f0_ceil = p.s.ceil;
-    bv.x_off = p.d_x_off; bv.y_off = p.d_y_off; bv.frame_off = p.d_frame_off; bv.nfft = p.d_nfft;
+    const BatchView bv = batch_view(p);
     auto mark = [&](int i) { if (marks_on) check(cudaEventRecord(marks[i], s), "cudaEventRecord"); };
     double* x = ptr<double>(p.at.x);
     double* y = ptr<double>(p.at.y);
     mark(0);
     check(cudaMemsetAsync(ptr<int>(p.at.flag), 0, 16, s), "memset");
     check(launch_check_finite(x, p.x_off[B], ptr<int>(p.at.flag), sms, s), "check_finite");
-    if (p.ratio > 1) {
-      DecimateView dv{};
-      dv.clips = B; dv.ratio = p.ratio; dv.lag = p.lag; dv.seg_len = kSegment;
-      std::memcpy(dv.a, kLowA[p.ratio], sizeof dv.a);
-      std::memcpy(dv.b, kLowB[p.ratio], sizeof dv.b);
-      std::memcpy(dv.trans, p.trans, sizeof dv.trans);
-      dv.x_off = p.d_x_off; dv.y_off = p.d_y_off; dv.t_off = p.d_t_off; dv.seg_off = p.d_seg_off;
-      check(launch_decimate(dv, x, ptr<double>(p.at.u), ptr<double>(p.at.states), p.total_seg, y, s),
-            "decimate");
-    } else {
-      check(launch_copy(x, p.x_off[B], y, s), "copy");
-    }
-    check(launch_remove_mean(bv, y, ptr<double>(p.at.bins), s), "remove_mean");
+    enqueue_waveform(p, x, s);
     mark(1);
     BankView kv{};
     kv.batch = bv;
@@ -625,15 +653,44 @@ struct Workspace {
                        ptr<double>(p.at.pruned), ptr<double>(p.at.pruned_scores), ptr<double>(p.at.best), s),
           "prune");
     mark(5);
-    ContourView cv{};
-    cv.batch = bv;
-    cv.pruned = ptr<double>(p.at.pruned); cv.pruned_scores = ptr<double>(p.at.pruned_scores);
-    cv.best = ptr<double>(p.at.best); cv.count = ptr<int>(p.at.count);
-    cv.scratch_off = p.d_scratch_off; cv.scratch = ptr<double>(p.at.scratch);
-    cv.smoothed = ptr<double>(p.at.smoothed); cv.period = p.s.period; cv.out_off = p.d_out_off;
-    cv.f0_out = ptr<double>(p.at.f0); cv.t_out = ptr<double>(p.at.times);
-    check(launch_contour(cv, s), "contour");
+    check(launch_contour(contour_view(p), s), "contour");
     mark(6);
+  }
+
+  // The tape of the F0 gradient for the run just enqueued on `s` (it reads
+  // that run's candidates and contour scratch).
+  void enqueue_tape(Plan& p, double* tape, cudaStream_t s) {
+    check(launch_tape(contour_view(p), ptr<double>(p.at.cand), p.frame_off[p.clips], tape, s), "tape");
+  }
+
+  // Backward pass of the F0 gradient: dL/dx for the clips at `x` from dL/df0
+  // and the forward pass's tape. The waveform y is recomputed from x; the
+  // adjoints run in reverse stage order.
+  void enqueue_backward(Plan& p, const double* x, const double* tape, const double* grad_f0, double* grad_x,
+                        cudaStream_t s) {
+    const int B = p.clips;
+    const int64_t F = p.frame_off[B];
+    const BatchView bv = batch_view(p);
+    enqueue_waveform(p, x, s);
+    GradView gv{};
+    gv.batch = bv;
+    gv.tape = tape;
+    gv.scratch_off = p.d_scratch_off; gv.scratch = ptr<double>(p.at.scratch);
+    gv.period = p.s.period; gv.out_off = p.d_out_off;
+    gv.grad_f0 = grad_f0;
+    gv.grad_fixed = ptr<double>(p.at.grad_fixed);
+    check(launch_contour_adjoint(gv, s), "contour_adjoint");
+    double* grad_y = ptr<double>(p.at.grad_y);
+    check(cudaMemsetAsync(grad_y, 0, 8 * p.y_off[B], s), "memset");
+    check(launch_refine_adjoint(bv, ptr<double>(p.at.y), tape, gv.grad_fixed, F, grad_y, sms, s),
+          "refine_adjoint");
+    check(launch_remove_mean_adjoint(bv, grad_y, s), "remove_mean_adjoint");
+    if (p.ratio > 1)
+      check(launch_decimate_adjoint(decimate_view(p), grad_y, ptr<double>(p.at.u), ptr<double>(p.at.states),
+                                    p.total_seg, grad_x, s),
+            "decimate_adjoint");
+    else
+      check(launch_copy(grad_y, p.x_off[B], grad_x, s), "copy");
   }
 
   // Runs the compute of `p` on stream `s`, through the plan's graph when
@@ -758,6 +815,16 @@ void run_host(const double* x, const int64_t* offsets, int clips, const Settings
   if (record) collect_stage_ms(ws);
 }
 
+// Settings and offsets of a batch, clip by clip.
+void validate_batch(const int64_t* offsets, int clips, int fs, double f0_floor, double f0_ceil,
+                    double frame_period) {
+  if (clips <= 0 || !offsets) throw InvalidArgument("a batch needs at least one clip and its offsets");
+  for (int c = 0; c < clips; ++c) {
+    if (offsets[c + 1] < offsets[c]) throw InvalidArgument("offsets must be nondecreasing");
+    validate_settings(offsets[c + 1] - offsets[c], fs, f0_floor, f0_ceil, frame_period);
+  }
+}
+
 // ---------------------------------------------- allocation-free decimation --
 // Scratch of hv_decimate_noalloc: a fixed array in the library's device
 // image, present on every GPU that loads the library for the life of the
@@ -869,12 +936,8 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
                      double f0_ceil, double frame_period, int device, double* f0, double* times,
                      unsigned flags, void* stream) {
   return guarded([&] {
-    if (clips <= 0 || !offsets) throw InvalidArgument("a batch needs at least one clip and its offsets");
+    validate_batch(offsets, clips, fs, f0_floor, f0_ceil, frame_period);
     if (!x || !f0) throw InvalidArgument("null buffer");
-    for (int c = 0; c < clips; ++c) {
-      if (offsets[c + 1] < offsets[c]) throw InvalidArgument("offsets must be nondecreasing");
-      validate_settings(offsets[c + 1] - offsets[c], fs, f0_floor, f0_ceil, frame_period);
-    }
     Settings s{fs, f0_floor, f0_ceil, frame_period};
     const bool record = (flags & HV_RECORD_STAGES) != 0;
     const bool use_graph = !(flags & HV_NO_GRAPH) && !record;
@@ -906,6 +969,53 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
       check(cudaStreamSynchronize(st), "harvest_batch");
       collect_stage_ms(ws);
     }
+  });
+}
+
+int hv_harvest_grad_forward(const double* x, const int64_t* offsets, int clips, int fs, double f0_floor,
+                            double f0_ceil, double frame_period, int device, double* f0, double* times,
+                            double* tape, void* stream) {
+  return guarded([&] {
+    validate_batch(offsets, clips, fs, f0_floor, f0_ceil, frame_period);
+    if (!x || !f0 || !tape) throw InvalidArgument("null buffer");
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    Plan& p = ws.plan_for(Settings{fs, f0_floor, f0_ceil, frame_period}, offsets, clips);
+    ws.ensure_arena(p.arena_bytes);
+    const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
+    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
+    check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyDeviceToDevice, st),
+          "cudaMemcpy(x)");
+    ws.run(p, st, true, false);
+    check(cudaMemcpyAsync(f0, ws.ptr<double>(p.at.f0), 8 * total_out, cudaMemcpyDeviceToDevice, st),
+          "cudaMemcpy(f0)");
+    if (times)
+      check(cudaMemcpyAsync(times, ws.ptr<double>(p.at.times), 8 * total_out, cudaMemcpyDeviceToDevice, st),
+            "cudaMemcpy(times)");
+    ws.enqueue_tape(p, tape, st);
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
+  });
+}
+
+int hv_harvest_grad_backward(const double* x, const int64_t* offsets, int clips, int fs, double f0_floor,
+                             double f0_ceil, double frame_period, int device, const double* tape,
+                             const double* grad_f0, double* grad_x, void* stream) {
+  return guarded([&] {
+    validate_batch(offsets, clips, fs, f0_floor, f0_ceil, frame_period);
+    if (!x || !tape || !grad_f0 || !grad_x) throw InvalidArgument("null buffer");
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    Plan& p = ws.plan_for(Settings{fs, f0_floor, f0_ceil, frame_period}, offsets, clips);
+    ws.ensure_arena(p.arena_bytes);
+    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
+    ws.enqueue_backward(p, x + offsets[0], tape, grad_f0, grad_x + offsets[0], st);
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
   });
 }
 

@@ -5,6 +5,23 @@
 
 namespace hv {
 
+// Candidate in column `col` of frame `gf` after overlap: column g*K + j of
+// frame f holds candidate j of frame f (g = 0), f - g (g = 1..3) or
+// f + g - 3 (g = 4..6); other columns are zero.
+__device__ __forceinline__ double overlapped_candidate(const BatchView& v, const double* cand,
+                                                       const int* count, int64_t gf, int col) {
+  int c = owner(v.frame_off, v.clips, gf);
+  int64_t row0 = v.frame_off[c];
+  int frames = static_cast<int>(v.frame_off[c + 1] - row0);
+  int f = static_cast<int>(gf - row0);
+  int k = count[c];
+  if (col >= 7 * k) return 0.0;
+  int g = col / k, j = col - g * k;
+  int src = g == 0 ? f : (g <= 3 ? f - g : f + (g - 3));
+  if (src < 0 || src >= frames) return 0.0;
+  return cand[(row0 + src) * v.per_group + j];
+}
+
 struct DecimateView {
   int clips;
   int ratio;
@@ -44,6 +61,21 @@ struct ContourView {
   const int64_t* out_off;       // [clips + 1]
   double* f0_out;
   double* t_out;
+};
+
+// The F0 gradient holds every discrete choice of the forward pass fixed.
+// Its tape has two doubles per 1 ms frame: the FixF0Contour step-3 value and,
+// where that value is nonzero, the initial candidate F0 whose refinement it
+// is (0 elsewhere).
+struct GradView {
+  BatchView batch;
+  const double* tape;           // [frames][2]
+  const int64_t* scratch_off;   // [clips + 1] in doubles, as ContourView
+  double* scratch;
+  double period;                // frame_period in ms
+  const int64_t* out_off;       // [clips + 1]
+  const double* grad_f0;        // [outputs] dL/df0
+  double* grad_fixed;           // [frames] dL/d(step-3 value)
 };
 
 cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, double* states,
@@ -101,6 +133,15 @@ cudaError_t launch_prune(const BatchView& v, const double* refined, const double
                          double* pruned_scores, double* best, cudaStream_t stream);
 
 int64_t contour_scratch(int64_t frames);
+cudaError_t launch_tape(const ContourView& v, const double* cand, int64_t total_frames, double* tape,
+                        cudaStream_t stream);
+cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream);
+cudaError_t launch_refine_adjoint(const BatchView& v, const double* y, const double* tape,
+                                  const double* grad_fixed, int64_t total_frames, double* grad_y, int sms,
+                                  cudaStream_t stream);
+cudaError_t launch_remove_mean_adjoint(const BatchView& v, double* grad_y, cudaStream_t stream);
+cudaError_t launch_decimate_adjoint(const DecimateView& v, const double* grad_y, double* u, double* states,
+                                    int64_t segments, double* grad_x, cudaStream_t stream);
 cudaError_t launch_contour(const ContourView& v, cudaStream_t stream);
 
 }  // namespace hv

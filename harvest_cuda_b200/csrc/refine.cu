@@ -21,23 +21,6 @@ __device__ __forceinline__ int size_class(int len) {
   return e < 2 ? 4 * e : 4 * e + ((len >> (e - 2)) & 3);
 }
 
-// Candidate in column `col` of frame `gf` after overlap: column g*K + j of
-// frame f holds candidate j of frame f (g = 0), f - g (g = 1..3) or
-// f + g - 3 (g = 4..6); other columns are zero.
-__device__ __forceinline__ double overlapped_candidate(const BatchView& v, const double* cand,
-                                                       const int* count, int64_t gf, int col) {
-  int c = owner(v.frame_off, v.clips, gf);
-  int64_t row0 = v.frame_off[c];
-  int frames = static_cast<int>(v.frame_off[c + 1] - row0);
-  int f = static_cast<int>(gf - row0);
-  int k = count[c];
-  if (col >= 7 * k) return 0.0;
-  int g = col / k, j = col - g * k;
-  int src = g == 0 ? f : (g <= 3 ? f - g : f + (g - 3));
-  if (src < 0 || src >= frames) return 0.0;
-  return cand[(row0 + src) * v.per_group + j];
-}
-
 template <bool kScatter>
 __global__ void __launch_bounds__(256)
 refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
@@ -98,41 +81,48 @@ __global__ void refine_offsets(const int* __restrict__ class_count, int* __restr
 // 2 pi k / n; both are re-anchored from exact values every kAnchor samples.
 constexpr int kAnchor = 64;
 
-__device__ void refine_candidate(const double* __restrict__ y, int y_len, double fs, double t,
-                                 double f0c, double f0_floor, double f0_ceil, double& out_f0,
-                                 double& out_score) {
-  const int half = static_cast<int>(1.5 * fs / f0c + 1.0);
-  const int len = 2 * half + 1;
-  const double span = (2.0 * half + 1.0) / fs;
-  const int n = 1 << (2 + (31 - __clz(len)));        // 2^(2 + floor(log2 len)), len odd
-  const int base = matlab_round((t + (-half) / fs) * fs + 0.001);
-  const int harmonics = imin(static_cast<int>(fs / 2.0 / f0c), 6);
+// The discrete parameters of one candidate's refinement: window half length,
+// FFT size, first waveform index and the harmonic bins.
+struct CandidateWindow {
+  int half, len, n, base, harmonics;
   int bin[6];
-  double mr[6], mi[6], dr[6], di[6], tr[6], ti[6], sr[6], si[6];
+  __device__ __forceinline__ CandidateWindow(double fs, double t, double f0c) {
+    half = static_cast<int>(1.5 * fs / f0c + 1.0);
+    len = 2 * half + 1;
+    n = 1 << (2 + (31 - __clz(len)));        // 2^(2 + floor(log2 len)), len odd
+    base = matlab_round((t + (-half) / fs) * fs + 0.001);
+    harmonics = imin(static_cast<int>(fs / 2.0 / f0c), 6);
 #pragma unroll
-  for (int h = 0; h < 6; ++h) {
-    bin[h] = h < harmonics ? matlab_round(f0c * n / fs * (h + 1)) : 0;
-    mr[h] = mi[h] = dr[h] = di[h] = 0.0;
-    sincospi(-2.0 * bin[h] / n, &si[h], &sr[h]);
+    for (int h = 0; h < 6; ++h) bin[h] = h < harmonics ? matlab_round(f0c * n / fs * (h + 1)) : 0;
   }
+};
+
+// Visits the window's samples in order: body(i, w, dw, tr, ti) receives the
+// Blackman window w, the centred difference window dw and, per harmonic,
+// the twiddle e^{-2 pi i bin i / n} as (tr, ti).
+template <class Body>
+__device__ __forceinline__ void walk_window(const CandidateWindow& cw, double fs, double t, Body&& body) {
+  const int len = cw.len, n = cw.n;
+  const double span = (2.0 * cw.half + 1.0) / fs;
+  double tr[6], ti[6], sr[6], si[6];
+#pragma unroll
+  for (int h = 0; h < 6; ++h) sincospi(-2.0 * cw.bin[h] / n, &si[h], &sr[h]);
   double ds, dc;
   sincospi(2.0 / len, &ds, &dc);
   // Window phase of sample i: 2 pi ((base + i - 1) / fs - t) / span, as in
   // GetMainWindow (harvest.cpp:449-455).
   auto phase = [&](int i, double& c1, double& s1) {
-    double tmp = (base + i - 1.0) / fs - t;
+    double tmp = (cw.base + i - 1.0) / fs - t;
     sincos(2.0 * kPi * tmp / span, &s1, &c1);
   };
   double nc, ns;
   phase(0, nc, ns);
   double w_prev = 0.0;
   double w_cur = 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0);
-  const bool inside = base - 1 >= 0 && base - 1 + len <= y_len;
-  const double* yb = y + (base - 1);
   for (int i0 = 0; i0 < len; i0 += kAnchor) {
 #pragma unroll
     for (int h = 0; h < 6; ++h) {
-      long long m = (static_cast<long long>(bin[h]) * i0) % n;
+      long long m = (static_cast<long long>(cw.bin[h]) * i0) % n;
       sincospi(-2.0 * static_cast<double>(m) / n, &ti[h], &tr[h]);
     }
     phase(i0 + 1, nc, ns);
@@ -140,14 +130,9 @@ __device__ void refine_candidate(const double* __restrict__ y, int y_len, double
     for (int i = i0; i < i1; ++i) {
       const double w_next = (i + 1 < len) ? 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0) : 0.0;
       const double dw = -(w_next - w_prev) / 2.0;
-      const double xs = inside ? yb[i] : y[imax(0, imin(y_len - 1, base + i - 1))];
-      const double a = xs * w_cur, d = xs * dw;
+      body(i, w_cur, dw, tr, ti);
 #pragma unroll
       for (int h = 0; h < 6; ++h) {
-        mr[h] = fma(a, tr[h], mr[h]);
-        mi[h] = fma(a, ti[h], mi[h]);
-        dr[h] = fma(d, tr[h], dr[h]);
-        di[h] = fma(d, ti[h], di[h]);
         const double r = fma(tr[h], sr[h], -ti[h] * si[h]);
         ti[h] = fma(tr[h], si[h], ti[h] * sr[h]);
         tr[h] = r;
@@ -159,22 +144,55 @@ __device__ void refine_candidate(const double* __restrict__ y, int y_len, double
       w_cur = w_next;
     }
   }
+}
+
+// Main- and difference-window spectra of one candidate at its harmonic bins
+// (GetSpectra, harvest.cpp:461-505, at those bins only).
+struct HarmonicSpectra {
+  double mr[6], mi[6], dr[6], di[6];
+};
+
+__device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, int y_len, double fs,
+                                                  double t, const CandidateWindow& cw, HarmonicSpectra& sp) {
+#pragma unroll
+  for (int h = 0; h < 6; ++h) sp.mr[h] = sp.mi[h] = sp.dr[h] = sp.di[h] = 0.0;
+  const bool inside = cw.base - 1 >= 0 && cw.base - 1 + cw.len <= y_len;
+  const double* yb = y + (cw.base - 1);
+  walk_window(cw, fs, t, [&](int i, double w, double dw, const double* tr, const double* ti) {
+    const double xs = inside ? yb[i] : y[imax(0, imin(y_len - 1, cw.base + i - 1))];
+    const double a = xs * w, d = xs * dw;
+#pragma unroll
+    for (int h = 0; h < 6; ++h) {
+      sp.mr[h] = fma(a, tr[h], sp.mr[h]);
+      sp.mi[h] = fma(a, ti[h], sp.mi[h]);
+      sp.dr[h] = fma(d, tr[h], sp.dr[h]);
+      sp.di[h] = fma(d, ti[h], sp.di[h]);
+    }
+  });
+}
+
+__device__ void refine_candidate(const double* __restrict__ y, int y_len, double fs, double t,
+                                 double f0c, double f0_floor, double f0_ceil, double& out_f0,
+                                 double& out_score) {
+  const CandidateWindow cw(fs, t, f0c);
+  HarmonicSpectra sp;
+  candidate_spectra(y, y_len, fs, t, cw, sp);
   // FixF0 (harvest.cpp:507-536), same evaluation order.
   double num = 0.0, den = 0.0, err = 0.0;
 #pragma unroll
   for (int h = 0; h < 6; ++h) {
-    if (h >= harmonics) break;
-    const double power = mr[h] * mr[h] + mi[h] * mi[h];
-    const double cross = mr[h] * di[h] - mi[h] * dr[h];
+    if (h >= cw.harmonics) break;
+    const double power = sp.mr[h] * sp.mr[h] + sp.mi[h] * sp.mi[h];
+    const double cross = sp.mr[h] * sp.di[h] - sp.mi[h] * sp.dr[h];
     const double inst =
-        power == 0.0 ? 0.0 : static_cast<double>(bin[h]) * fs / n + cross / power * fs / 2.0 / kPi;
+        power == 0.0 ? 0.0 : static_cast<double>(cw.bin[h]) * fs / cw.n + cross / power * fs / 2.0 / kPi;
     const double amp = sqrt(power);
     num += amp * inst;
     den += amp * (h + 1.0);
     err += fabs((inst / (h + 1.0) - f0c) / f0c);
   }
   double refined = num / (den + kGuard);
-  double score = 1.0 / (err / harmonics + kGuard);
+  double score = 1.0 / (err / cw.harmonics + kGuard);
   if (refined < f0_floor || refined > f0_ceil || score < 2.5) refined = score = 0.0;  // :610-614
   out_f0 = refined;
   out_score = score;
@@ -200,6 +218,75 @@ refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restri
   }
 }
 
+// Adjoint of the refinement for the F0 gradient, with every discrete choice
+// held fixed. For each frame whose FixF0Contour step-3 value is a refined
+// candidate, FixF0's result f = sum_h A_h IF_h / (sum_h (h + 1) A_h + guard),
+// with A_h = |M_h| and IF_h = bin_h fs / n + (Mr Di - Mi Dr) / |M_h|^2 fs / 2 pi,
+// is differentiated through the main and difference spectra M_h, D_h, which
+// are linear in the waveform. The spectra are recomputed from y and the
+// candidate F0 on the tape (nothing per frame is stored by the forward
+// pass); the frame's share of dL/dy is added with atomics.
+__global__ void __launch_bounds__(128)
+refine_adjoint(BatchView v, const double* __restrict__ y, const double* __restrict__ tape,
+               const double* __restrict__ grad_fixed, int64_t total_frames, double* __restrict__ grad_y) {
+  for (int64_t gf = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gf < total_frames;
+       gf += (int64_t)gridDim.x * blockDim.x) {
+    const double g = grad_fixed[gf];
+    const double f0c = tape[2 * gf + 1];
+    // A tape from the forward pass holds candidates within [f0_floor, f0_ceil];
+    // anything outside [1, fs_r] Hz is not one and is skipped.
+    if (g == 0.0 || !(f0c >= 1.0 && f0c <= v.fs_r)) continue;
+    const int c = owner(v.frame_off, v.clips, gf);
+    const int f = static_cast<int>(gf - v.frame_off[c]);
+    const int64_t y0 = v.y_off[c];
+    const int y_len = static_cast<int>(v.y_off[c + 1] - y0);
+    const double fs = v.fs_r, t = f * 1 / 1000.0;
+    const CandidateWindow cw(fs, t, f0c);
+    HarmonicSpectra sp;
+    candidate_spectra(y + y0, y_len, fs, t, cw, sp);
+    double num = 0.0, den = 0.0, amp[6], inst[6];
+#pragma unroll
+    for (int h = 0; h < 6; ++h) {
+      amp[h] = inst[h] = 0.0;
+      if (h >= cw.harmonics) continue;
+      const double power = sp.mr[h] * sp.mr[h] + sp.mi[h] * sp.mi[h];
+      const double cross = sp.mr[h] * sp.di[h] - sp.mi[h] * sp.dr[h];
+      inst[h] = power == 0.0 ? 0.0 : static_cast<double>(cw.bin[h]) * fs / cw.n + cross / power * fs / 2.0 / kPi;
+      amp[h] = sqrt(power);
+      num += amp[h] * inst[h];
+      den += amp[h] * (h + 1.0);
+    }
+    const double e = den + kGuard, refined = num / e, kappa = fs / 2.0 / kPi;
+    // g * df/dMr_h, df/dMi_h, df/dDr_h, df/dDi_h.
+    double cmr[6], cmi[6], cdr[6], cdi[6];
+#pragma unroll
+    for (int h = 0; h < 6; ++h) {
+      cmr[h] = cmi[h] = cdr[h] = cdi[h] = 0.0;
+      const double power = amp[h] * amp[h];
+      if (h >= cw.harmonics || !(amp[h] > 0.0)) continue;
+      const double cross = sp.mr[h] * sp.di[h] - sp.mi[h] * sp.dr[h];
+      const double g_amp = (inst[h] - refined * (h + 1.0)) / e;
+      const double g_inst = amp[h] / e;
+      const double g_power = g_amp / (2.0 * amp[h]) - g_inst * kappa * cross / (power * power);
+      const double g_cross = g_inst * kappa / power;
+      cmr[h] = g * (2.0 * sp.mr[h] * g_power + sp.di[h] * g_cross);
+      cmi[h] = g * (2.0 * sp.mi[h] * g_power - sp.dr[h] * g_cross);
+      cdr[h] = -g * sp.mi[h] * g_cross;
+      cdi[h] = g * sp.mr[h] * g_cross;
+    }
+    double* gy = grad_y + y0;
+    walk_window(cw, fs, t, [&](int i, double w, double dw, const double* tr, const double* ti) {
+      double sm = 0.0, sd = 0.0;
+#pragma unroll
+      for (int h = 0; h < 6; ++h) {
+        sm += cmr[h] * tr[h] + cmi[h] * ti[h];
+        sd += cdr[h] * tr[h] + cdi[h] * ti[h];
+      }
+      atomicAdd(gy + imax(0, imin(y_len - 1, cw.base + i - 1)), w * sm + dw * sd);
+    });
+  }
+}
+
 cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const double* y,
                           const double* cand, const int* count, int64_t total_frames, double* refined,
                           double* scores, int sms, cudaStream_t stream) {
@@ -215,6 +302,15 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
   refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, total_frames, b.class_count,
                                                 b.class_cursor, b.jobs);
   refine_jobs<<<sms * 16, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refine_adjoint(const BatchView& v, const double* y, const double* tape,
+                                  const double* grad_fixed, int64_t total_frames, double* grad_y, int sms,
+                                  cudaStream_t stream) {
+  const int64_t blocks = (total_frames + 127) / 128;
+  refine_adjoint<<<static_cast<unsigned>(blocks < sms * 8 ? blocks : sms * 8), 128, 0, stream>>>(
+      v, y, tape, grad_fixed, total_frames, grad_y);
   return cudaGetLastError();
 }
 

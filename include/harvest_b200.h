@@ -90,6 +90,32 @@ HV_API int hv_profile(const double* x, int64_t n, int fs, double f0_floor, doubl
                double frame_period, int device, double* f0, double* times, int64_t out_len,
                double* stage_ms);
 
+/* F0 gradient (no reference counterpart; the reference has no derivative).
+ * Harvest is piecewise smooth in x: with every discrete choice of a forward
+ * pass held fixed (candidates kept, voicing, FixF0Contour's choices, the
+ * section boundaries), the output F0 is a smooth function of the waveform
+ * through the refined candidates' spectra, FixStep4's gap fills, the
+ * smoothing filter and the resampling.
+ *
+ * hv_harvest_grad_forward is hv_harvest_batch on device pointers that also
+ * writes `tape` (device memory, 2 doubles per 1 ms analysis frame, i.e.
+ * hv_output_length(n, fs, 1.0) frames per clip, clips in order): the
+ * FixF0Contour step-3 F0 and the initial candidate F0 it was refined from.
+ * hv_harvest_grad_backward takes the same x, offsets and settings, that tape
+ * and dL/df0 (device, laid out like f0) and writes dL/dx (device, laid out
+ * like x); it recomputes the decimated waveform and the spectra rather than
+ * storing them. Both order their work on `stream`; NULL is the legacy
+ * default stream (PyTorch's default stream), not the engine's own stream.
+ * Contributions of overlapping refinement windows are added with atomics,
+ * so dL/dx is reproducible to rounding, not bit for bit. */
+HV_API int hv_harvest_grad_forward(const double* x, const int64_t* offsets, int clips, int fs,
+                                   double f0_floor, double f0_ceil, double frame_period, int device,
+                                   double* f0, double* times, double* tape, void* stream);
+HV_API int hv_harvest_grad_backward(const double* x, const int64_t* offsets, int clips, int fs,
+                                    double f0_floor, double f0_ceil, double frame_period, int device,
+                                    const double* tape, const double* grad_f0, double* grad_x,
+                                    void* stream);
+
 /* Diagnostic: runs hv_harvest on one clip and copies the intermediate stage
  * buffers to host memory, for stage-by-stage parity tests. Any pointer may
  * be NULL. Shapes (row-major, frames = analysis frames on the 1 ms grid,
