@@ -20,6 +20,12 @@ pass of the whole Harvest pipeline over that batch.
 * ``cpu_baseline``: the reference's bundled WORLD Harvest (oracle/_ref) on
   the host cores over a bounded sample of the same batch.
 
+* ``grad``: the F0 gradient (``harvest_cuda_b200.autograd``) on 32 clips of
+  4 s at 16 kHz from the same generator, L = sum over voiced frames of
+  (f0 - true f0)^2: forward + backward device milliseconds per audio second
+  (CUDA events), and the agreement of dL/dx with central finite differences
+  (eps 1e-6) at 64 random samples per clip.
+
 ``--impl reference`` times that CPU implementation alone on the host cores
 and prints the same line with ``"impl": "reference"``.
 """
@@ -60,6 +66,7 @@ def parse_args():
                     help="target duration of the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-clip", action="store_true")
+    ap.add_argument("--no-grad", action="store_true", help="skip the F0-gradient measurement")
     ap.add_argument("--clips", type=int, default=0,
                     help="use only the first N clips of the workload (small profiling runs)")
     return ap.parse_args()
@@ -382,6 +389,8 @@ def run_ours(args):
         if world == 1 and not args.no_per_clip:
             line["per_clip"] = per_clip(hv, wl, local)
             line["batched_over_per_clip"] = round(e2e["value"] / line["per_clip"]["value"], 2)
+        if world == 1 and not args.no_grad:
+            line["grad"] = grad_measure(hv, args.steps, max(3, args.warmup), stream)
         if pool is not None:
             sample = cpu_sample(wl, args.cpu_seconds, cores)
             a, wall, kind = run_cpu(pool, wl, sample)
@@ -455,6 +464,93 @@ def summarize(args, wl, value, ms, stages, e2e, clocks, device, world):
         "gpu_launches": kernels_per_step(ratio) * args.steps,
         "model_bytes_per_step": byte_model(wl["lengths"], wl["fs"], wl["floor"], wl["ceil"],
                                            wl["period"]),
+    }
+
+
+def grad_measure(hv, steps, warmup, stream, fd_per_clip=64, eps=1e-6):
+    """F0-gradient forward + backward time per audio second on 32 x 4 s
+    clips at 16 kHz, and dL/dx against central finite differences of the
+    GPU forward pass."""
+    import torch
+    from harvest_cuda_b200 import autograd, signals
+    w = signals.workload("grad32x4s_16k", seed=7)
+    fs, floor, ceil, period = w["fs"], w["f0_floor"], w["f0_ceil"], w["frame_period"]
+    clips, truths = w["clips"], w["truths"]
+    offsets = tuple(int(v) for v in np.concatenate([[0], np.cumsum([len(c) for c in clips])]))
+    audio = offsets[-1] / fs
+    x = torch.from_numpy(np.concatenate(clips)).cuda()
+    counts = [hv.output_length(len(c), fs, period) for c in clips]
+    times = np.concatenate([np.arange(n) * period / 1000.0 for n in counts])
+    target_np = np.concatenate([tr(t) for tr, t in zip(truths, np.split(times, np.cumsum(counts)[:-1]))])
+    target = torch.from_numpy(target_np).cuda()
+
+    def step():
+        xs = x.detach().requires_grad_(True)
+        f0, _ = autograd.HarvestF0.apply(xs, offsets, fs, floor, ceil, period)
+        voiced = (f0.detach() > 0) & (target > 0)
+        loss = ((f0 - target) ** 2 * voiced).sum()
+        return xs, f0, loss
+
+    for _ in range(warmup):
+        xs, f0, loss = step()
+        loss.backward()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd = bwd = 0.0
+    for _ in range(steps):
+        ev[0].record(stream)
+        xs, f0, loss = step()
+        ev[1].record(stream)
+        loss.backward()
+        ev[2].record(stream)
+        torch.cuda.synchronize()
+        fwd += ev[0].elapsed_time(ev[1])
+        bwd += ev[1].elapsed_time(ev[2])
+    fwd, bwd = fwd / steps, bwd / steps
+    # Finite differences of the forward pass at random samples.
+    grad = xs.grad.cpu().numpy()
+    f0n = f0.detach().cpu().numpy()
+    rng = np.random.default_rng(0)
+    g, fd, scale, switched, flipped = [], [], [], 0, 0
+    o = np.concatenate([[0], np.cumsum(counts)])
+    for c, clip in enumerate(clips):
+        base_f0, tgt = f0n[o[c]:o[c + 1]], target_np[o[c]:o[c + 1]]
+        voiced = (base_f0 > 0) & (tgt > 0)
+        positions = rng.choice(len(clip), fd_per_clip, replace=False)
+        batch = []
+        for p in positions:
+            for s in (eps, -eps):
+                xp = clip.copy()
+                xp[p] += s
+                batch.append(xp)
+        out = hv.harvest_many(batch, fs, floor, ceil, period)
+        for k, p in enumerate(positions):
+            up, down = out[2 * k][0], out[2 * k + 1][0]
+            if not (np.array_equal(up > 0, base_f0 > 0) and np.array_equal(down > 0, base_f0 > 0)):
+                flipped += 1
+                continue
+            # L differences frame by frame: (a - t)^2 - (b - t)^2 = (a - b)(a + b - 2t).
+            central = np.sum(((up - down) * (up + down - 2 * tgt))[voiced]) / (2 * eps)
+            curvature = np.sum(((up - base_f0) * (up + base_f0 - 2 * tgt) -
+                                (base_f0 - down) * (base_f0 + down - 2 * tgt))[voiced]) / eps
+            if abs(curvature) > 1e-3 * max(abs(central), 1.0):
+                switched += 1
+                continue
+            g.append(grad[offsets[c] + p])
+            fd.append(central)
+            scale.append(np.abs(grad[offsets[c]:offsets[c + 1]]).max())
+    g, fd, scale = np.array(g), np.array(fd), np.array(scale)
+    return {
+        "metric": "F0-grad fwd+bwd ms/s", "value": (fwd + bwd) / audio, "unit": "ms per audio-s",
+        "higher_is_better": False, "fwd_ms": fwd, "bwd_ms": bwd, "steps": steps,
+        "workload": "32 clips x 4 s at 16 kHz (glide generator), floor 71, ceil 800, period 5 ms",
+        "audio_seconds": audio,
+        "finite_differences": {
+            "eps": eps, "samples": int(g.size), "voicing_flips": flipped, "candidate_switches": switched,
+            "rel_error_norm": float(np.linalg.norm(g - fd) / np.linalg.norm(fd)),
+            "rel_error_max": float(np.max(np.abs(g - fd) / scale)),
+            "rel_error_note": "norm-wise over the samples; max is per sample |g - fd| over the "
+                              "clip's max |dL/dx| (difference noise at eps 1e-6 is ~1e-6 absolute)"},
     }
 
 
