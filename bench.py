@@ -340,10 +340,13 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # --- value: device-resident batch, replayed graph, CUDA events.
+    # --- value: device-resident batch, replayed graph, CUDA events. The first
+    # warm-up call autotunes the refinement launch shape for this batch.
     for _ in range(max(3, args.warmup)):
         device_step()
     torch.cuda.synchronize()
+    tuning = (ct.c_int * 3)()
+    _native.raise_for(_native.lib.hv_last_tuning(tuning))
     barrier()
     torch.cuda.synchronize()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -375,17 +378,23 @@ def run_ours(args):
     x_host = pinned.numpy()
     hv.harvest_batch(x_host, offsets, fs, floor, ceil, period, device=local)
     barrier()
+    laps = []
     t0 = time.perf_counter()
     for _ in range(args.steps):
         f0, times, _ = hv.harvest_batch(x_host, offsets, fs, floor, ceil, period, device=local)
+        laps.append(time.perf_counter())
     e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
     barrier()
+    laps = np.diff(np.concatenate([[t0], laps])) * 1000.0
     e2e = {"value": audio * world / e2e_s, "unit": "audio-s/s",
-           "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(f0.nbytes + times.nbytes)}
+           "h2d_bytes_per_step": int(x_host.nbytes), "d2h_bytes_per_step": int(f0.nbytes + times.nbytes),
+           "ms_per_step": e2e_s * 1000.0, "ms_min": float(laps.min()), "ms_median": float(np.median(laps))}
 
     line = None
     if rank == 0:
         line = summarize(args, wl, value, ms, stages, e2e, clocks.summary(), local, world)
+        line["config"]["autotuned"] = {"refine_min_blocks_per_sm": tuning[0], "refine_grid_blocks_per_sm": tuning[1],
+                                       "key": "fs, f0 range, log2 of the batch's samples"}
         if world == 1 and not args.no_per_clip:
             line["per_clip"] = per_clip(hv, wl, local)
             line["batched_over_per_clip"] = round(e2e["value"] / line["per_clip"]["value"], 2)

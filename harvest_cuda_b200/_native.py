@@ -35,6 +35,7 @@ SIGNATURES = {
                                     ct.c_void_p]),
     "hv_stage_name": (ct.c_char_p, [ct.c_int]),
     "hv_last_stage_ms": (ct.c_int, [_D]),
+    "hv_last_tuning": (ct.c_int, [ct.POINTER(ct.c_int)]),
     "hv_profile": (ct.c_int, [_D, ct.c_int64, ct.c_int, ct.c_double, ct.c_double, ct.c_double,
                               ct.c_int, _D, _D, ct.c_int64, _D]),
     "hv_harvest_stages": (ct.c_int, [_D, ct.c_int64, ct.c_int, ct.c_double, ct.c_double, ct.c_int,

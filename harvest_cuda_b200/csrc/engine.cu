@@ -15,6 +15,7 @@
 #include <atomic>
 #include <climits>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <list>
@@ -23,6 +24,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "harvest_b200.h"
@@ -34,6 +36,7 @@ namespace {
 // ---------------------------------------------------------------- errors --
 thread_local std::string g_error;
 thread_local double g_stage_ms[HV_STAGE_COUNT] = {};
+thread_local int g_tuning[3] = {0, 0, 0};   // refinement shape of the last call, and whether it tuned
 
 struct InvalidArgument : std::runtime_error { using std::runtime_error::runtime_error; };
 struct RuntimeFailure : std::runtime_error { using std::runtime_error::runtime_error; };
@@ -110,12 +113,17 @@ void check_device(int device) {
   if (device >= count)
     throw InvalidArgument("device " + std::to_string(device) + " is out of range; " +
                           std::to_string(count) + " GPU(s) are visible through CUDA_VISIBLE_DEVICES");
-  cudaDeviceProp p{};
-  check(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
-  if (p.major < 10)
+  // One attribute query: cudaGetDeviceProperties fills every property
+  // through the driver and took milliseconds (at times over 100 ms) per call.
+  int major = 0;
+  check(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "cudaDeviceGetAttribute");
+  if (major < 10) {
+    cudaDeviceProp p{};
+    check(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
     throw RuntimeFailure("this build targets sm_100a (B200); device " + std::to_string(device) +
                          " (" + p.name + ") has compute capability " + std::to_string(p.major) +
                          "." + std::to_string(p.minor));
+  }
 }
 
 // Keeps a device's primary context retained while its workspace lives.
@@ -298,6 +306,9 @@ struct Plan {
   int* d_half;
   double *d_centre, *d_taps;
   int2* d_items;
+  // Refinement launch shape, chosen by the autotuner on the plan's first run.
+  RefineShape refine_shape;
+  bool tuned = false;
   // Captured launch sequence for this plan at a given arena base.
   cudaGraphExec_t graph = nullptr;
   void* graph_arena = nullptr;
@@ -332,6 +343,9 @@ struct Workspace {
   double2* twiddles = nullptr;  // e^{-2 pi i t / 8192}, t < 8192
   int* host_flag = nullptr;      // pinned word for the non-finite-sample flag
   std::map<Settings, std::shared_ptr<const BankTables>> banks;
+  // Autotuned refinement shapes by (fs, f0_floor, f0_ceil, log2 of the
+  // batch's total samples).
+  std::map<std::tuple<int, double, double, int>, RefineShape> tuned_shapes;
   std::list<std::unique_ptr<Plan>> plans;  // most recent first
 
   explicit Workspace(int dev) : device(dev), ctx(dev) {
@@ -646,7 +660,7 @@ struct Workspace {
     rb.total = rb.class_cursor + kRefineClasses;
     rb.jobs = ptr<RefineJob>(p.at.jobs);
     check(launch_refine(bv, rb, y, ptr<double>(p.at.cand), ptr<int>(p.at.count), F,
-                        ptr<double>(p.at.refined), ptr<double>(p.at.scores), sms, s),
+                        ptr<double>(p.at.refined), ptr<double>(p.at.scores), sms, p.refine_shape, s),
           "refine");
     mark(4);
     check(launch_prune(bv, ptr<double>(p.at.refined), ptr<double>(p.at.scores), ptr<int>(p.at.count), F,
@@ -693,9 +707,75 @@ struct Workspace {
       check(launch_copy(grad_y, p.x_off[B], grad_x, s), "copy");
   }
 
+  // Autotuner: picks the refinement launch shape for the
+  // plan's key the first time a plan with that key runs. It runs the
+  // pipeline once to produce the refinement's inputs, then times the
+  // refinement stage alone under every candidate shape (each launched twice,
+  // the second timed, so that lazy module loading is not timed) and keeps the
+  // fastest. All shapes give bit-identical results, so tuning never changes
+  // an output. HARVEST_B200_AUTOTUNE=0 skips it and uses the default shape.
+  void autotune(Plan& p, cudaStream_t s) {
+    p.tuned = true;
+    int64_t total = p.x_off[p.clips];
+    int bucket = 0;
+    while ((int64_t(2) << bucket) <= total) ++bucket;
+    const auto key = std::make_tuple(p.s.fs, p.s.floor, p.s.ceil, bucket);
+    g_tuning[2] = 0;
+    // HARVEST_B200_REFINE_SHAPE=min_blocks,blocks_per_sm forces a shape.
+    if (const char* forced = std::getenv("HARVEST_B200_REFINE_SHAPE")) {
+      int a = 0, b = 0;
+      if (std::sscanf(forced, "%d,%d", &a, &b) == 2 && (a == 1 || a == 4 || a == 5) && b >= 1 && b <= 1024) {
+        p.refine_shape = RefineShape{a, b};
+        return;
+      }
+    }
+    auto it = tuned_shapes.find(key);
+    if (it != tuned_shapes.end()) {
+      p.refine_shape = it->second;
+      return;
+    }
+    const char* env = std::getenv("HARVEST_B200_AUTOTUNE");
+    if (env && !std::strcmp(env, "0")) {
+      p.refine_shape = RefineShape{};
+      return;
+    }
+    enqueue(p, s, false);
+    const BatchView bv = batch_view(p);
+    RefineBuffers rb{};
+    rb.class_count = ptr<int>(p.at.classes);
+    rb.class_cursor = rb.class_count + kRefineClasses;
+    rb.total = rb.class_cursor + kRefineClasses;
+    rb.jobs = ptr<RefineJob>(p.at.jobs);
+    const int64_t F = p.frame_off[p.clips];
+    RefineShape best{};
+    float best_ms = 0.0f;
+    for (int min_blocks : {1, 4, 5})
+      for (int per_sm : {16, 32, 64}) {
+        RefineShape shape{min_blocks, per_sm};
+        for (int rep = 0; rep < 2; ++rep) {
+          check(cudaEventRecord(marks[0], s), "cudaEventRecord");
+          check(launch_refine(bv, rb, ptr<double>(p.at.y), ptr<double>(p.at.cand), ptr<int>(p.at.count), F,
+                              ptr<double>(p.at.refined), ptr<double>(p.at.scores), sms, shape, s),
+                "refine");
+          check(cudaEventRecord(marks[1], s), "cudaEventRecord");
+        }
+        check(cudaEventSynchronize(marks[1]), "cudaEventSynchronize");
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, marks[0], marks[1]), "cudaEventElapsedTime");
+        if (best_ms == 0.0f || ms < best_ms) { best_ms = ms; best = shape; }
+      }
+    tuned_shapes[key] = best;
+    p.refine_shape = best;
+    g_tuning[2] = 1;
+  }
+
   // Runs the compute of `p` on stream `s`, through the plan's graph when
   // allowed. Inputs are in the arena's x region; outputs land in f0/times.
   void run(Plan& p, cudaStream_t s, bool use_graph, bool marks_on) {
+    if (!p.tuned) autotune(p, s);
+    else g_tuning[2] = 0;
+    g_tuning[0] = p.refine_shape.min_blocks;
+    g_tuning[1] = p.refine_shape.blocks_per_sm;
     if (!use_graph || marks_on) {
       enqueue(p, s, marks_on);
       return;
@@ -878,9 +958,12 @@ int hv_cuda_available(int device) {
   int count = 0;
   if (cudaGetDeviceCount(&count) != cudaSuccess) { cudaGetLastError(); return 0; }
   if (device >= count) return 0;
-  cudaDeviceProp p{};
-  if (cudaGetDeviceProperties(&p, device) != cudaSuccess) { cudaGetLastError(); return 0; }
-  return p.major >= 10 ? 1 : 0;
+  int major = 0;
+  if (cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return major >= 10 ? 1 : 0;
 }
 
 int64_t hv_output_length(int64_t n, int fs, double frame_period) {
@@ -925,6 +1008,13 @@ int hv_last_stage_ms(double* stage_ms) {
   return guarded([&] {
     if (!stage_ms) throw InvalidArgument("null buffer");
     std::memcpy(stage_ms, g_stage_ms, sizeof g_stage_ms);
+  });
+}
+
+int hv_last_tuning(int* shape) {
+  return guarded([&] {
+    if (!shape) throw InvalidArgument("null buffer");
+    std::memcpy(shape, g_tuning, sizeof g_tuning);
   });
 }
 

@@ -125,9 +125,18 @@ struct RefineBuffers {
   int* total;          // [1]
   RefineJob* jobs;     // [frames * capacity]
 };
+// Launch shape of the refinement jobs: minimum resident 128-thread blocks per
+// SM the kernel instance is compiled for (1, 4 or 5; fewer registers per
+// thread for more blocks) and grid blocks per SM. Every shape computes the
+// same values bit for bit.
+struct RefineShape {
+  int min_blocks = 4;
+  int blocks_per_sm = 32;
+};
+
 cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const double* y,
                           const double* cand, const int* count, int64_t total_frames, double* refined,
-                          double* scores, int sms, cudaStream_t stream);
+                          double* scores, int sms, RefineShape shape, cudaStream_t stream);
 cudaError_t launch_prune(const BatchView& v, const double* refined, const double* scores,
                          const int* count, int64_t total_frames, double* pruned,
                          double* pruned_scores, double* best, cudaStream_t stream);

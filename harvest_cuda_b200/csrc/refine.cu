@@ -152,23 +152,87 @@ struct HarmonicSpectra {
   double mr[6], mi[6], dr[6], di[6];
 };
 
+// The bin sums are Goertzel recurrences in Reinsch's form, which keeps the
+// error near that of a direct sum for angles near 0 (and, in its mirrored
+// form, near pi): with theta = 2 pi bin / n,
+//   cos theta >= 0:  q += lambda s + x,  s += q,   lambda = -4 sin^2(theta / 2)
+//   cos theta <  0:  q  = lambda s - q + x,  s = q - s,  lambda = 4 cos^2(theta / 2)
+// written as q = lambda s + sigma q + x, s = sigma s + q with sigma = +-1.
+// After the window, s_{N-1} = s and s_{N-2} = sigma (s - q), and
+// X = e^{-i theta (N-1)} (s_{N-1} - e^{-i theta} s_{N-2}). Per harmonic and
+// sample this is 3 operations per windowed sequence, against 4 accumulations
+// and a 4-operation twiddle rotation for the direct sum.
 __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, int y_len, double fs,
                                                   double t, const CandidateWindow& cw, HarmonicSpectra& sp) {
+  const int len = cw.len, n = cw.n;
+  double lam[6], sig[6], qa[6], sa[6], qd[6], sd[6];
 #pragma unroll
-  for (int h = 0; h < 6; ++h) sp.mr[h] = sp.mi[h] = sp.dr[h] = sp.di[h] = 0.0;
-  const bool inside = cw.base - 1 >= 0 && cw.base - 1 + cw.len <= y_len;
-  const double* yb = y + (cw.base - 1);
-  walk_window(cw, fs, t, [&](int i, double w, double dw, const double* tr, const double* ti) {
-    const double xs = inside ? yb[i] : y[imax(0, imin(y_len - 1, cw.base + i - 1))];
-    const double a = xs * w, d = xs * dw;
-#pragma unroll
-    for (int h = 0; h < 6; ++h) {
-      sp.mr[h] = fma(a, tr[h], sp.mr[h]);
-      sp.mi[h] = fma(a, ti[h], sp.mi[h]);
-      sp.dr[h] = fma(d, tr[h], sp.dr[h]);
-      sp.di[h] = fma(d, ti[h], sp.di[h]);
+  for (int h = 0; h < 6; ++h) {
+    const double frac = static_cast<double>(cw.bin[h]) / n;      // theta / (2 pi)
+    if (4 * cw.bin[h] <= n) {
+      const double half = sinpi(frac);
+      lam[h] = -4.0 * half * half;
+      sig[h] = 1.0;
+    } else {
+      const double half = cospi(frac);
+      lam[h] = 4.0 * half * half;
+      sig[h] = -1.0;
     }
-  });
+    qa[h] = sa[h] = qd[h] = sd[h] = 0.0;
+  }
+  const double span = (2.0 * cw.half + 1.0) / fs;
+  double ds, dc;
+  sincospi(2.0 / len, &ds, &dc);
+  auto phase = [&](int i, double& c1, double& s1) {
+    double tmp = (cw.base + i - 1.0) / fs - t;
+    sincos(2.0 * kPi * tmp / span, &s1, &c1);
+  };
+  double nc, ns;
+  phase(0, nc, ns);
+  double w_prev = 0.0;
+  double w_cur = 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0);
+  const bool inside = cw.base - 1 >= 0 && cw.base - 1 + len <= y_len;
+  const double* yb = y + (cw.base - 1);
+  for (int i0 = 0; i0 < len; i0 += kAnchor) {
+    phase(i0 + 1, nc, ns);
+    const int i1 = imin(i0 + kAnchor, len);
+    for (int i = i0; i < i1; ++i) {
+      const double w_next = (i + 1 < len) ? 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0) : 0.0;
+      const double dw = -(w_next - w_prev) / 2.0;
+      const double xs = inside ? yb[i] : y[imax(0, imin(y_len - 1, cw.base + i - 1))];
+      const double a = xs * w_cur, d = xs * dw;
+#pragma unroll
+      for (int h = 0; h < 6; ++h) {
+        qa[h] = fma(lam[h], sa[h], fma(sig[h], qa[h], a));
+        sa[h] = fma(sig[h], sa[h], qa[h]);
+        qd[h] = fma(lam[h], sd[h], fma(sig[h], qd[h], d));
+        sd[h] = fma(sig[h], sd[h], qd[h]);
+      }
+      const double rc = fma(nc, dc, -ns * ds);
+      ns = fma(nc, ds, ns * dc);
+      nc = rc;
+      w_prev = w_cur;
+      w_cur = w_next;
+    }
+  }
+#pragma unroll
+  for (int h = 0; h < 6; ++h) {
+    double st, ct, sp_, cp;
+    sincospi(2.0 * cw.bin[h] / n, &st, &ct);
+    const long long m = (static_cast<long long>(cw.bin[h]) * (len - 1)) % n;
+    sincospi(-2.0 * static_cast<double>(m) / n, &sp_, &cp);
+    // a sequence
+    double s2 = sig[h] * (sa[h] - qa[h]);
+    double re = sa[h] - ct * s2, im = st * s2;
+    sp.mr[h] = re * cp - im * sp_;
+    sp.mi[h] = re * sp_ + im * cp;
+    // d sequence
+    s2 = sig[h] * (sd[h] - qd[h]);
+    re = sd[h] - ct * s2;
+    im = st * s2;
+    sp.dr[h] = re * cp - im * sp_;
+    sp.di[h] = re * sp_ + im * cp;
+  }
 }
 
 __device__ void refine_candidate(const double* __restrict__ y, int y_len, double fs, double t,
@@ -199,7 +263,10 @@ __device__ void refine_candidate(const double* __restrict__ y, int y_len, double
 }
 
 // One thread per job, grid-stride over the job list (longest windows first).
-__global__ void __launch_bounds__(128)
+// kMinBlocks caps registers so that that many 128-thread blocks fit on an
+// SM; the autotuner picks the instance and the grid (RefineShape).
+template <int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks)
 refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restrict__ jobs,
             const int* __restrict__ total, double* __restrict__ refined, double* __restrict__ scores) {
   const int count = *total;
@@ -289,7 +356,7 @@ refine_adjoint(BatchView v, const double* __restrict__ y, const double* __restri
 
 cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const double* y,
                           const double* cand, const int* count, int64_t total_frames, double* refined,
-                          double* scores, int sms, cudaStream_t stream) {
+                          double* scores, int sms, RefineShape shape, cudaStream_t stream) {
   const int64_t cells = total_frames * v.capacity;
   cudaError_t e;
   if ((e = cudaMemsetAsync(b.class_count, 0, sizeof(int) * kRefineClasses, stream)) != cudaSuccess) return e;
@@ -301,7 +368,12 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
   refine_offsets<<<1, 32, 0, stream>>>(b.class_count, b.class_cursor, b.total);
   refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, total_frames, b.class_count,
                                                 b.class_cursor, b.jobs);
-  refine_jobs<<<sms * 16, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores);
+  const unsigned job_grid = static_cast<unsigned>(sms * shape.blocks_per_sm);
+  switch (shape.min_blocks) {
+    case 4: refine_jobs<4><<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores); break;
+    case 5: refine_jobs<5><<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores); break;
+    default: refine_jobs<1><<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores); break;
+  }
   return cudaGetLastError();
 }
 

@@ -90,6 +90,17 @@ HV_API int hv_profile(const double* x, int64_t n, int fs, double f0_floor, doubl
                double frame_period, int device, double* f0, double* times, int64_t out_len,
                double* stage_ms);
 
+/* Refinement launch shape of the calling thread's last Harvest call (no
+ * reference counterpart). The engine autotunes it once per (fs, f0_floor,
+ * f0_ceil, log2 of the batch's total samples) on each device, the first time
+ * a batch with that key runs, by timing every candidate shape on that
+ * batch; all shapes give bit-identical results. shape[0]: minimum resident
+ * 128-thread blocks per SM of the kernel instance (1, 4 or 5), shape[1]:
+ * grid blocks per SM (16, 32 or 64), shape[2]: 1 if that call ran the
+ * tuning, else 0. HARVEST_B200_AUTOTUNE=0 in the environment turns tuning
+ * off (shape 4, 32). */
+HV_API int hv_last_tuning(int* shape);
+
 /* F0 gradient (no reference counterpart; the reference has no derivative).
  * Harvest is piecewise smooth in x: with every discrete choice of a forward
  * pass held fixed (candidates kept, voicing, FixF0Contour's choices, the
