@@ -52,6 +52,7 @@ WORKLOADS = {
     "batch64_48k": "64 clips x U(2,30) s at 48 kHz, floor 71, ceil 800, period 1 ms",
     "clip60s_44k": "1 clip of 60 s at 44.1 kHz, floor 71, ceil 800, period 5 ms",
     "clip3s_16k": "1 clip of 3 s at 16 kHz, floor 71, ceil 800, period 5 ms",
+    "grad32x4s_16k": "F0 gradient only: 32 clips x 4 s at 16 kHz, floor 71, ceil 800, period 5 ms",
 }
 
 
@@ -67,6 +68,10 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-clip", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the F0-gradient measurement")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="with --impl reference: skip timing the reference's own CUDA path")
+    ap.add_argument("--grad-fd-samples", type=int, default=64,
+                    help="random samples per clip for the finite-difference check (0: none)")
     ap.add_argument("--clips", type=int, default=0,
                     help="use only the first N clips of the workload (small profiling runs)")
     return ap.parse_args()
@@ -254,6 +259,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    if args.workload == "grad32x4s_16k":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no F0 gradient"}), flush=True)
+        return
     cores = os.cpu_count() or 1
     wl = make_workload(args.workload, seed=1000, clips=args.clips)
     pool = mp.get_context("spawn").Pool(cores)
@@ -281,11 +289,60 @@ def run_reference(args):
         "e2e": {"value": value, "unit": "audio-s/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if not args.no_reference_cuda:
+        line["reference_cuda"] = reference_cuda_measure(wl)
     print(json.dumps(line), flush=True)
 
 
+def reference_cuda_measure(wl, budget_s=60.0):
+    """The reference's own GPU path (oracle/_ref/libref_cuda.so, its
+    src/cuda_backend.cu + src/engine.cpp) on the workload's clips, one clip per
+    call as its API takes them, host arrays in and out; wall clock over
+    consecutive clips until all are done or `budget_s` has passed."""
+    import oracle
+    ref = oracle.reference_cuda()
+    if ref is None:
+        return {"unavailable": "oracle/_ref/libref_cuda.so was not built"}
+    if not ref.available(0):
+        return {"unavailable": "the reference's CUDA build does not run on device 0"}
+    offs, x = wl["offsets"], wl["packed"]
+    clips = [np.ascontiguousarray(x[offs[i]:offs[i + 1]]) for i in range(len(offs) - 1)]
+    for c in clips[:3]:
+        ref.harvest(c, wl["fs"], wl["floor"], wl["ceil"], wl["period"])
+    done = audio = 0
+    t0 = time.perf_counter()
+    for c in clips:
+        ref.harvest(c, wl["fs"], wl["floor"], wl["ceil"], wl["period"])
+        done += 1
+        audio += len(c) / wl["fs"]
+        if time.perf_counter() - t0 > budget_s:
+            break
+    wall = time.perf_counter() - t0
+    return {"value": audio / wall, "unit": "audio-s/s", "clips": done, "audio_seconds": audio,
+            "wall_s": wall, "path": "reference src/cuda_backend.cu + src/engine.cpp analyze(), "
+                                    "per clip, host buffers, built for sm_100a by oracle/Makefile"}
+
+
 # ------------------------------------------------------------ our arm --
+def run_grad_only(args):
+    """--workload grad32x4s_16k: the F0-gradient measurement as the line."""
+    import torch
+    import harvest_cuda_b200 as hv
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    g = grad_measure(hv, args.steps, max(3, args.warmup), stream, fd_per_clip=args.grad_fd_samples)
+    line = {"metric": g.pop("metric"), "value": g.pop("value"), "unit": g.pop("unit"), "n_gpus": 1,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": g["fwd_ms"] + g["bwd_ms"],
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
+            "grad": g}
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args):
+    if args.workload == "grad32x4s_16k":
+        run_grad_only(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -399,7 +456,8 @@ def run_ours(args):
             line["per_clip"] = per_clip(hv, wl, local)
             line["batched_over_per_clip"] = round(e2e["value"] / line["per_clip"]["value"], 2)
         if world == 1 and not args.no_grad:
-            line["grad"] = grad_measure(hv, args.steps, max(3, args.warmup), stream)
+            line["grad"] = grad_measure(hv, args.steps, max(3, args.warmup), stream,
+                                        fd_per_clip=args.grad_fd_samples)
         if pool is not None:
             sample = cpu_sample(wl, args.cpu_seconds, cores)
             a, wall, kind = run_cpu(pool, wl, sample)
@@ -522,7 +580,7 @@ def grad_measure(hv, steps, warmup, stream, fd_per_clip=64, eps=1e-6):
     rng = np.random.default_rng(0)
     g, fd, scale, switched, flipped = [], [], [], 0, 0
     o = np.concatenate([[0], np.cumsum(counts)])
-    for c, clip in enumerate(clips):
+    for c, clip in enumerate(clips if fd_per_clip > 0 else []):
         base_f0, tgt = f0n[o[c]:o[c + 1]], target_np[o[c]:o[c + 1]]
         voiced = (base_f0 > 0) & (tgt > 0)
         positions = rng.choice(len(clip), fd_per_clip, replace=False)
@@ -549,17 +607,20 @@ def grad_measure(hv, steps, warmup, stream, fd_per_clip=64, eps=1e-6):
             fd.append(central)
             scale.append(np.abs(grad[offsets[c]:offsets[c + 1]]).max())
     g, fd, scale = np.array(g), np.array(fd), np.array(scale)
+    fd_report = None
+    if g.size:
+        fd_report = {
+            "eps": eps, "samples": int(g.size), "voicing_flips": flipped, "candidate_switches": switched,
+            "rel_error_norm": float(np.linalg.norm(g - fd) / np.linalg.norm(fd)),
+            "rel_error_max": float(np.max(np.abs(g - fd) / scale)),
+            "rel_error_note": "norm-wise over the samples; max is per sample |g - fd| over the "
+                              "clip's max |dL/dx| (difference noise at eps 1e-6 is ~1e-6 absolute)"}
     return {
         "metric": "F0-grad fwd+bwd ms/s", "value": (fwd + bwd) / audio, "unit": "ms per audio-s",
         "higher_is_better": False, "fwd_ms": fwd, "bwd_ms": bwd, "steps": steps,
         "workload": "32 clips x 4 s at 16 kHz (glide generator), floor 71, ceil 800, period 5 ms",
         "audio_seconds": audio,
-        "finite_differences": {
-            "eps": eps, "samples": int(g.size), "voicing_flips": flipped, "candidate_switches": switched,
-            "rel_error_norm": float(np.linalg.norm(g - fd) / np.linalg.norm(fd)),
-            "rel_error_max": float(np.max(np.abs(g - fd) / scale)),
-            "rel_error_note": "norm-wise over the samples; max is per sample |g - fd| over the "
-                              "clip's max |dL/dx| (difference noise at eps 1e-6 is ~1e-6 absolute)"},
+        "finite_differences": fd_report,
     }
 
 

@@ -4,10 +4,15 @@
 * ``reference()``: the reference's own bundled WORLD Harvest compiled from the
   reference sources by ``Makefile`` into ``_ref/libworld_ref.so``; ``None``
   when that library was never built.
+* ``reference_cuda()``: the reference's own CUDA path (its
+  ``src/cuda_backend.cu`` + ``src/engine.cpp``) compiled by ``Makefile`` into
+  ``_ref/libref_cuda.so``; ``None`` when absent. It runs on the GPU and serves
+  as a second parity reference and the timed reference GPU path.
 
-Only tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
-``bench.py`` import this package, and only as the checker or the timed CPU
-baseline. The engine under ``harvest_cuda_b200`` never does.
+Only tests, ``__graft_entry__.smoke()`` and the reference legs of ``bench.py``
+(its CPU baseline and ``--impl reference``) import this package, and only as
+the checker or the timed reference. The engine under ``harvest_cuda_b200``
+never does.
 """
 from __future__ import annotations
 
@@ -20,6 +25,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_LIB = os.path.join(HERE, "liboracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libworld_ref.so")
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libref_cuda.so")
 
 _D = ct.POINTER(ct.c_double)
 _I = ct.POINTER(ct.c_int)
@@ -126,3 +132,33 @@ def reference():
 def best():
     """The reference build when present, else the restatement."""
     return reference() or port()
+
+
+class ReferenceCuda:
+    """The reference's own GPU Harvest (one clip per call, as its API)."""
+
+    def __init__(self, path):
+        self.lib = ct.CDLL(path)
+        self.lib.refcuda_last_error.restype = ct.c_char_p
+        self.lib.refcuda_available.argtypes = [ct.c_int]
+        self.lib.refcuda_harvest.argtypes = [_D, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                             ct.c_double, ct.c_int, _D, _D, ct.c_int]
+
+    def available(self, device=0):
+        return bool(self.lib.refcuda_available(int(device)))
+
+    def harvest(self, x, fs, f0_floor=71.0, f0_ceil=800.0, frame_period=5.0, device=0):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        m = int(1000.0 * len(x) / fs / frame_period) + 1
+        f0, t = np.zeros(m), np.zeros(m)
+        rc = self.lib.refcuda_harvest(_ptr(x), len(x), int(fs), float(f0_floor), float(f0_ceil),
+                                      float(frame_period), int(device), _ptr(f0), _ptr(t), m)
+        if rc != 0:
+            raise RuntimeError(self.lib.refcuda_last_error().decode())
+        return f0, t
+
+
+def reference_cuda():
+    if "ref_cuda" not in _cache:
+        _cache["ref_cuda"] = ReferenceCuda(REF_CUDA_LIB) if os.path.exists(REF_CUDA_LIB) else None
+    return _cache["ref_cuda"]
