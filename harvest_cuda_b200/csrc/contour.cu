@@ -52,25 +52,52 @@ __device__ int warp_boundary_list(F f, int len, int* out) {
   return count;
 }
 
-// SelectBestF0 (harvest.cpp:636-650).
-__device__ __forceinline__ double select_best(double ref, const double* cand, int count,
-                                              double allowed) {
-  double best = 0.0, err = allowed;
-  for (int i = 0; i < count; ++i) {
-    double e = fabs(ref - cand[i]) / ref;
-    if (e > err) continue;
-    best = cand[i];
-    err = e;
+// The contour stage runs one warp per clip and is bound by the latency of
+// dependent loads, so the sequential loops below load kChunk values ahead
+// into registers and then consume them in the reference's order.
+constexpr int kChunk = 8;
+
+// SelectBestF0 (harvest.cpp:636-650) with the columns spread over the lanes
+// of a warp. The
+// reference's loop keeps a candidate whenever its error is at most the
+// running minimum (which starts at `allowed`), so it returns the candidate
+// of smallest error, the later column on ties, or 0 if none is within
+// `allowed`; the warp arg-min below picks the same one. Every lane returns it.
+__device__ __forceinline__ double warp_select_best(double ref, const double* cand, int count,
+                                                   double allowed) {
+  const int lane = threadIdx.x & 31;
+  double best_e = allowed, best_v = 0.0;
+  int best_i = -1;
+  for (int i = lane; i < count; i += 32) {
+    const double c = cand[i];
+    const double e = fabs(ref - c) / ref;
+    if (e <= best_e) { best_e = e; best_i = i; best_v = c; }
   }
-  return best;
+  for (int o = 16; o; o >>= 1) {
+    const double oe = __shfl_xor_sync(kAll, best_e, o), ov = __shfl_xor_sync(kAll, best_v, o);
+    const int oi = __shfl_xor_sync(kAll, best_i, o);
+    if (oi >= 0 && (best_i < 0 || oe < best_e || (oe == best_e && oi > best_i))) {
+      best_e = oe; best_i = oi; best_v = ov;
+    }
+  }
+  return best_v;
 }
 
 // SearchScore (harvest.cpp:901-907).
 __device__ __forceinline__ double search_score(double f0, const double* cand, const double* score,
                                                int count) {
   double s = 0.0;
-  for (int i = 0; i < count; ++i)
-    if (f0 == cand[i] && s < score[i]) s = score[i];
+  for (int i0 = 0; i0 < count; i0 += kChunk) {
+    double c[kChunk], v[kChunk];
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k) {
+      c[k] = i0 + k < count ? cand[i0 + k] : 0.0;
+      v[k] = i0 + k < count ? score[i0 + k] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < kChunk; ++k)
+      if (i0 + k < count && f0 == c[k] && s < v[k]) s = v[k];
+  }
   return s;
 }
 
@@ -101,31 +128,72 @@ struct Butter {
 // Smooths the voiced section [st, ed] of the padded contour (lag 300) as
 // FilteringF0 does over the whole padded length: the held head, the body
 // and the held tail forward, then everything backward. Body outputs go to
-// out[j - lag]. The forward tail is stored in `tail` (capacity `cap`) until
-// its state stops changing; returns false if it did not within `cap`.
+// out[j - lag]. The forward tail runs until its state stops changing (or to
+// the end); the backward pass needs its outputs in reverse, so the forward
+// pass keeps the filter state every `cap` / 2 steps in the second half of
+// `tail` and the backward pass recomputes each stretch from its checkpoint
+// into the first half, newest first. Recomputation from a saved state
+// repeats the same steps, so this equals storing every output. Returns false
+// if the tail needs more than cap / 4 checkpoints.
 template <class P>
 __device__ bool smooth_section(P padded, int st, int ed, int64_t len, double* out, double* tail,
                                int64_t cap) {
   const int lag = 300;
   const double head = padded(st), tail_value = padded(ed);
+  constexpr int kAhead = 2 * kChunk;
   Butter fw;
   fw.run_constant(head, st);
-  for (int j = st; j <= ed; ++j) out[j - lag] = fw.step(padded(j));
+  for (int j0 = st; j0 <= ed; j0 += kAhead) {
+    double in[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) in[k] = j0 + k <= ed ? padded(j0 + k) : 0.0;
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k)
+      if (j0 + k <= ed) out[j0 + k - lag] = fw.step(in[k]);
+  }
   const int64_t trailing = len - 1 - ed;
-  int64_t stored = 0;
+  const int64_t stretch = cap / 2;
+  double* saved = tail + stretch;          // (w0, w1) before steps 0, stretch, 2 stretch, ...
+  int64_t stored = 0;                      // tail outputs before the state settled
   double settled = 0.0;
   bool fixed = false;
   for (int64_t k = 0; k < trailing; ++k) {
+    if (stored % stretch == 0) {
+      const int64_t c = stored / stretch;
+      if (2 * c + 1 >= stretch) return false;
+      saved[2 * c] = fw.w0;
+      saved[2 * c + 1] = fw.w1;
+    }
     double p0 = fw.w0, p1 = fw.w1;
     double o = fw.step(tail_value);
     if (fw.w0 == p0 && fw.w1 == p1) { settled = o; fixed = true; break; }
-    if (stored == cap) return false;
-    tail[stored++] = o;
+    ++stored;
   }
   Butter bw;
   if (fixed) bw.run_constant(settled, trailing - stored);
-  for (int64_t k = stored - 1; k >= 0; --k) bw.step(tail[k]);
-  for (int j = ed; j >= st; --j) out[j - lag] = bw.step(out[j - lag]);
+  for (int64_t first = (stored > 0 ? (stored - 1) / stretch : -1) * stretch; first >= 0; first -= stretch) {
+    const int64_t n = stored - first < stretch ? stored - first : stretch;
+    Butter re;
+    re.w0 = saved[2 * (first / stretch)];
+    re.w1 = saved[2 * (first / stretch) + 1];
+    for (int64_t k = 0; k < n; ++k) tail[k] = re.step(tail_value);
+    for (int64_t k0 = n - 1; k0 >= 0; k0 -= kAhead) {
+      double in[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) in[k] = k0 - k >= 0 ? tail[k0 - k] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k)
+        if (k0 - k >= 0) bw.step(in[k]);
+    }
+  }
+  for (int j0 = ed; j0 >= st; j0 -= kAhead) {
+    double in[kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) in[k] = j0 - k >= st ? out[j0 - k - lag] : 0.0;
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k)
+      if (j0 - k >= st) out[j0 - k - lag] = bw.step(in[k]);
+  }
   return true;
 }
 
@@ -174,26 +242,28 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
   }
   __syncwarp();
   for (int i = lane; i < F; i += 32) s3[i] = s2[i];
-  // FixStep3 (harvest.cpp:968-995): Extend/ExtendF0 per section in parallel.
+  // FixStep3 (harvest.cpp:968-995): Extend/ExtendF0, one section at a time
+  // with the whole warp (each frame's SelectBestF0 across the lanes).
   nb = warp_boundary_list([&](int i) { return s2[i]; }, F, bl);
   const int sections = imin(nb / 2, static_cast<int>(sections_cap));
-  for (int i = lane; i < sections; i += 32) {
+  for (int i = 0; i < sections; ++i) {
     const int st = bl[2 * i], ed = bl[2 * i + 1];
     double* fwd = ext + (2 * i) * kExtend;
     double* bwd = fwd + kExtend;
-    for (int k = 0; k < kExtend; ++k) fwd[k] = bwd[k] = 0.0;
+    for (int k = lane; k < kExtend; k += 32) fwd[k] = bwd[k] = 0.0;
+    __syncwarp();
     {  // ExtendF0 forward from the end (harvest.cpp:867-870)
       const int last = imin(F - 2, ed + 100);
       double cur = s2[ed];
       int reached = ed, misses = 0;
       for (int k = 0; k <= last - ed; ++k) {
         const int idx = ed + k + 1;
-        const double val = select_best(cur, cand + static_cast<int64_t>(idx) * stride, columns, 0.18);
-        fwd[k] = val;
+        const double val = warp_select_best(cur, cand + static_cast<int64_t>(idx) * stride, columns, 0.18);
+        if (lane == 0) fwd[k] = val;
         if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
         if (misses == 4) break;
       }
-      sec[8 * i + 3] = reached;
+      if (lane == 0) sec[8 * i + 3] = reached;
     }
     {  // ExtendF0 backward from the start (harvest.cpp:871-873)
       const int last = imax(1, st - 100);
@@ -201,15 +271,17 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
       int reached = st, misses = 0;
       for (int k = 0; k <= st - last; ++k) {
         const int idx = st - k - 1;
-        const double val = select_best(cur, cand + static_cast<int64_t>(idx) * stride, columns, 0.18);
-        bwd[k] = val;
+        const double val = warp_select_best(cur, cand + static_cast<int64_t>(idx) * stride, columns, 0.18);
+        if (lane == 0) bwd[k] = val;
         if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
         if (misses == 4) break;
       }
-      sec[8 * i + 2] = reached;
+      if (lane == 0) sec[8 * i + 2] = reached;
     }
-    sec[8 * i + 0] = st;
-    sec[8 * i + 1] = ed;
+    if (lane == 0) {
+      sec[8 * i + 0] = st;
+      sec[8 * i + 1] = ed;
+    }
   }
   __syncwarp();
   // A section's extended row: its body from s2 plus the extension values.
@@ -220,19 +292,31 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
     if (j < st && st - 1 - j < kExtend) return ext[(2 * i + 1) * kExtend + (st - 1 - j)];
     return 0.0;
   };
-  // ExtendSub (harvest.cpp:840-856) and MakeSortedOrder (harvest.cpp:883-896)
-  // in lane 0: the running mean is never reset; kept sections keep their
-  // order, their extended bounds go to bl[2k], bl[2k+1], the section index to
-  // sec[8k + 4] and the sort order to sec[8k + 5].
+  // ExtendSub (harvest.cpp:840-856): the running mean is never reset. The
+  // lanes load 32 channel values at a time and every lane adds them in
+  // order from shuffles, so all lanes hold the reference's sum. Kept
+  // sections keep their order; their section index goes to sec[8k + 4].
   int kept = 0;
-  if (lane == 0) {
+  {
     double mean = 0.0;
     for (int i = 0; i < sections; ++i) {
       const int st = sec[8 * i + 2], ed = sec[8 * i + 3];
-      for (int j = st; j < ed; ++j) mean += channel(i, j);
+      for (int j0 = st; j0 < ed; j0 += 32) {
+        const double v = j0 + lane < ed ? channel(i, j0 + lane) : 0.0;
+        const int m = imin(32, ed - j0);
+        for (int k = 0; k < m; ++k) mean += __shfl_sync(kAll, v, k);
+      }
       mean /= ed - st;
-      if (2200.0 / mean < ed - st) sec[8 * kept++ + 4] = i;
+      if (2200.0 / mean < ed - st) {
+        if (lane == 0) sec[8 * kept + 4] = i;
+        ++kept;
+      }
     }
+  }
+  __syncwarp();
+  // MakeSortedOrder (harvest.cpp:883-896) in lane 0: extended bounds of the
+  // kept sections go to bl[2k], bl[2k+1] and the sort order to sec[8k + 5].
+  if (lane == 0) {
     for (int k = 0; k < kept; ++k) {
       const int i = sec[8 * k + 4];
       bl[2 * k] = sec[8 * i + 2];
@@ -246,7 +330,6 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
         else break;
       }
   }
-  kept = __shfl_sync(kAll, kept, 0);
   __syncwarp();
   if (kept != 0) {
     // MergeF0 (harvest.cpp:937-963): start from the first kept section, then
@@ -256,34 +339,41 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
     for (int j = lane; j < F; j += 32) s3[j] = channel(first, j);
     __syncwarp();
     for (int i = 1; i < kept; ++i) {
-      int from = 0, to = -1, ch = 0;
-      if (lane == 0) {
-        const int o = sec[8 * i + 5];
-        ch = sec[8 * o + 4];
-        const int st2 = bl[2 * o], ed2 = bl[2 * o + 1];
-        if (st2 - bl[1] > 0) {
-          from = st2; to = ed2;
-          bl[0] = st2;
-          bl[1] = ed2;
-        } else {
-          const int st1 = bl[0], ed1 = bl[1];
-          if (!(st1 <= st2 && ed1 >= ed2)) {   // MergeF0Sub (harvest.cpp:912-932)
-            double sc1 = 0.0, sc2 = 0.0;
-            for (int j = st2; j <= ed1; ++j) {
-              sc1 += search_score(s3[j], cand + static_cast<int64_t>(j) * stride,
-                                  score + static_cast<int64_t>(j) * stride, columns);
-              sc2 += search_score(channel(ch, j), cand + static_cast<int64_t>(j) * stride,
-                                  score + static_cast<int64_t>(j) * stride, columns);
-            }
-            from = sc1 > sc2 ? ed1 : st2;
-            to = ed2;
-            bl[1] = ed2;
+      const int o = sec[8 * i + 5];
+      const int ch = sec[8 * o + 4];
+      const int st2 = bl[2 * o], ed2 = bl[2 * o + 1];
+      const int st1 = bl[0], ed1 = bl[1];
+      int from = 0, to = -1;
+      if (st2 - ed1 > 0) {
+        from = st2;
+        to = ed2;
+      } else if (!(st1 <= st2 && ed1 >= ed2)) {   // MergeF0Sub (harvest.cpp:912-932)
+        // Scores of 32 frames at a time, one per lane, summed in order by
+        // every lane from shuffles.
+        double sc1 = 0.0, sc2 = 0.0;
+        for (int j0 = st2; j0 <= ed1; j0 += 32) {
+          const int j = j0 + lane;
+          double a = 0.0, b = 0.0;
+          if (j <= ed1) {
+            a = search_score(s3[j], cand + static_cast<int64_t>(j) * stride,
+                             score + static_cast<int64_t>(j) * stride, columns);
+            b = search_score(channel(ch, j), cand + static_cast<int64_t>(j) * stride,
+                             score + static_cast<int64_t>(j) * stride, columns);
+          }
+          const int m = imin(32, ed1 - j0 + 1);
+          for (int k = 0; k < m; ++k) {
+            sc1 += __shfl_sync(kAll, a, k);
+            sc2 += __shfl_sync(kAll, b, k);
           }
         }
+        from = sc1 > sc2 ? ed1 : st2;
+        to = ed2;
       }
-      from = __shfl_sync(kAll, from, 0);
-      to = __shfl_sync(kAll, to, 0);
-      ch = __shfl_sync(kAll, ch, 0);
+      __syncwarp();
+      if (lane == 0 && to >= 0) {
+        if (st2 - ed1 > 0) bl[0] = st2;
+        bl[1] = ed2;
+      }
       for (int j = from + lane; j <= to; j += 32) s3[j] = channel(ch, j);
       __syncwarp();
     }

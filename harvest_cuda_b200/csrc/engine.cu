@@ -290,22 +290,26 @@ struct Plan {
   int fft_valid = 0;
   std::vector<int64_t> blk_off;
   int64_t total_blocks = 0;
-  double2* filters = nullptr;  // [bands][4097] filter spectra (own allocation)
-  int64_t* d_blk_off = nullptr;
-  // Device copy of all tables (one allocation) and arena layout.
-  void* meta = nullptr;
+  // Per-plan tables (offsets, work items, block offsets), uploaded to the
+  // head of the arena by Workspace::prepare when another plan used it last.
+  uint64_t id = 0;
+  std::vector<char> meta;
+  size_t o_x = 0, o_y = 0, o_t = 0, o_s = 0, o_f = 0, o_o = 0, o_sc = 0, o_n = 0, o_it = 0, o_bo = 0;
   size_t arena_bytes = 0;
   struct Layout {
-    size_t x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores, pruned,
-        pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed;
+    size_t meta, x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores,
+        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed;
   } at{};
   int bank_ctas = 0;
-  // Device pointers into `meta`.
+  // Device pointers, set by Workspace::prepare: into the arena's copy of
+  // `meta`, and into the workspace's device copy of the band tables.
   int64_t *d_x_off, *d_y_off, *d_t_off, *d_seg_off, *d_frame_off, *d_out_off, *d_scratch_off, *d_tap_off;
   int* d_nfft;
   int* d_half;
   double *d_centre, *d_taps;
   int2* d_items;
+  int64_t* d_blk_off = nullptr;
+  double2* filters = nullptr;  // [bands][4097] filter spectra of the FFT bank
   // Refinement launch shape, chosen by the autotuner on the plan's first run.
   RefineShape refine_shape;
   bool tuned = false;
@@ -314,7 +318,24 @@ struct Plan {
   void* graph_arena = nullptr;
   ~Plan() {
     if (graph) cudaGraphExecDestroy(graph);
-    if (meta) cudaFree(meta);
+  }
+};
+
+// Device copy of one (fs, f0_floor, f0_ceil)'s band tables and, once the FFT
+// bank needs them, its filter spectra; shared by every plan with those
+// settings, so that planning a new batch shape allocates nothing on the device.
+struct DeviceBank {
+  void* tables = nullptr;
+  double2* filters = nullptr;       // [bands][block / 2 + 1]
+  double* centre = nullptr;
+  int* half = nullptr;
+  int64_t* tap_off = nullptr;
+  double* taps = nullptr;
+  DeviceBank() = default;
+  DeviceBank(const DeviceBank&) = delete;
+  DeviceBank& operator=(const DeviceBank&) = delete;
+  ~DeviceBank() {
+    if (tables) cudaFree(tables);
     if (filters) cudaFree(filters);
   }
 };
@@ -347,6 +368,9 @@ struct Workspace {
   // batch's total samples).
   std::map<std::tuple<int, double, double, int>, RefineShape> tuned_shapes;
   std::list<std::unique_ptr<Plan>> plans;  // most recent first
+  std::map<Settings, std::unique_ptr<DeviceBank>> device_banks;
+  uint64_t next_plan_id = 1;
+  uint64_t meta_owner = 0;   // plan whose tables are at the head of the arena
 
   explicit Workspace(int dev) : device(dev), ctx(dev) {
     ContextGuard g(ctx.get());
@@ -365,6 +389,7 @@ struct Workspace {
       if (last) cudaEventSynchronize(last);
       if (stream) cudaStreamSynchronize(stream);
       plans.clear();
+      device_banks.clear();
       if (arena) cudaFree(arena);
       if (twiddles) cudaFree(twiddles);
       if (host_flag) cudaFreeHost(host_flag);
@@ -385,9 +410,92 @@ struct Workspace {
     for (auto& p : plans) {
       if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
     }
-    size_t grow = bytes + bytes / 8;
+    // Headroom of min(size, 512 MB): a run of calls with growing lengths
+    // reallocates a few times, and a large batch adds little on top.
+    size_t grow = bytes + std::min<size_t>(bytes, size_t(512) << 20);
+    meta_owner = 0;
     check(cudaMalloc(&arena, grow), "cudaMalloc(workspace)");
     arena_size = grow;
+  }
+
+  // The device band tables of `s`, with filter spectra when `spectra`.
+  DeviceBank& device_bank(const Settings& s, const BankTables& bank, bool spectra) {
+    Settings key{s.fs, s.floor, s.ceil, 0.0};
+    auto it = device_banks.find(key);
+    if (it == device_banks.end()) {
+      if (device_banks.size() >= 16) {
+        // Bounded: once the GPU is done, drop every bank and the graphs that
+        // captured their addresses (plans take the pointers anew each call).
+        check(cudaEventSynchronize(last), "cudaEventSynchronize");
+        check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
+        for (auto& q : plans)
+          if (q->graph) { cudaGraphExecDestroy(q->graph); q->graph = nullptr; }
+        device_banks.clear();
+      }
+      auto b = std::make_unique<DeviceBank>();
+      std::vector<char> blob;
+      auto put = [&](const void* src, size_t bytes) {
+        size_t at = align_up(blob.size());
+        blob.resize(at + bytes);
+        if (bytes) std::memcpy(blob.data() + at, src, bytes);
+        return at;
+      };
+      size_t o_c = put(bank.centre.data(), 8 * bank.centre.size());
+      size_t o_h = put(bank.half.data(), 4 * bank.half.size());
+      size_t o_to = put(bank.tap_off.data(), 8 * bank.tap_off.size());
+      size_t o_tp = put(bank.taps_rev.data(), 8 * bank.taps_rev.size());
+      check(cudaMalloc(&b->tables, blob.size()), "cudaMalloc(bank)");
+      check(cudaMemcpy(b->tables, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy(bank)");
+      char* m = static_cast<char*>(b->tables);
+      b->centre = reinterpret_cast<double*>(m + o_c);
+      b->half = reinterpret_cast<int*>(m + o_h);
+      b->tap_off = reinterpret_cast<int64_t*>(m + o_to);
+      b->taps = reinterpret_cast<double*>(m + o_tp);
+      it = device_banks.emplace(key, std::move(b)).first;
+    }
+    DeviceBank& b = *it->second;
+    if (spectra && !b.filters) {
+      if (fft_bank_ctas_per_sm() < 1) throw RuntimeFailure("FFT band-bank kernel does not fit on this device");
+      const int block = fft_bank_block_length();
+      check(cudaMalloc(&b.filters, sizeof(double2) * (block / 2 + 1) * bank.bands), "cudaMalloc(filters)");
+      check(launch_filter_spectra(b.half, b.tap_off, b.taps, bank.bands, bank.max_half, twiddles, b.filters,
+                                  stream),
+            "filter_spectra");
+      check(cudaStreamSynchronize(stream), "filter_spectra");
+    }
+    return b;
+  }
+
+  // Plan lookup, arena sizing, ordering after the previous call on `st`, and
+  // the plan's tables at the head of the arena (uploaded only when another
+  // plan used the arena last). Every entry point goes through here.
+  Plan& prepare(const Settings& s, const int64_t* offsets, int clips, cudaStream_t st) {
+    Plan& p = plan_for(s, offsets, clips);
+    ensure_arena(p.arena_bytes);
+    check(cudaStreamWaitEvent(st, last, 0), "cudaStreamWaitEvent");
+    if (meta_owner != p.id) {
+      check(cudaMemcpyAsync(ptr<char>(p.at.meta), p.meta.data(), p.meta.size(), cudaMemcpyHostToDevice, st),
+            "cudaMemcpy(plan)");
+      meta_owner = p.id;
+    }
+    char* m = ptr<char>(p.at.meta);
+    p.d_x_off = reinterpret_cast<int64_t*>(m + p.o_x);
+    p.d_y_off = reinterpret_cast<int64_t*>(m + p.o_y);
+    p.d_t_off = reinterpret_cast<int64_t*>(m + p.o_t);
+    p.d_seg_off = reinterpret_cast<int64_t*>(m + p.o_s);
+    p.d_frame_off = reinterpret_cast<int64_t*>(m + p.o_f);
+    p.d_out_off = reinterpret_cast<int64_t*>(m + p.o_o);
+    p.d_scratch_off = reinterpret_cast<int64_t*>(m + p.o_sc);
+    p.d_nfft = reinterpret_cast<int*>(m + p.o_n);
+    p.d_items = reinterpret_cast<int2*>(m + p.o_it);
+    p.d_blk_off = reinterpret_cast<int64_t*>(m + p.o_bo);
+    DeviceBank& b = device_bank(s, *p.bank, p.use_fft);
+    p.d_centre = b.centre;
+    p.d_half = b.half;
+    p.d_tap_off = b.tap_off;
+    p.d_taps = b.taps;
+    p.filters = b.filters;
+    return p;
   }
 
   std::shared_ptr<const BankTables> bank_for(const Settings& s) {
@@ -494,50 +602,26 @@ struct Workspace {
       }
       std::memcpy(p->trans, R, sizeof R);
     }
-    // Device metadata.
-    std::vector<char> blob;
+    // Per-plan tables, uploaded to the head of the arena by prepare().
+    p->id = next_plan_id++;
     auto put = [&](const void* src, size_t bytes) {
-      size_t at = align_up(blob.size());
-      blob.resize(at + bytes);
-      if (bytes) std::memcpy(blob.data() + at, src, bytes);
+      size_t at = align_up(p->meta.size());
+      p->meta.resize(at + bytes);
+      if (bytes) std::memcpy(p->meta.data() + at, src, bytes);
       return at;
     };
-    size_t o_x = put(p->x_off.data(), 8 * (B + 1)), o_y = put(p->y_off.data(), 8 * (B + 1));
-    size_t o_t = put(p->t_off.data(), 8 * (B + 1)), o_s = put(p->seg_off.data(), 8 * (B + 1));
-    size_t o_f = put(p->frame_off.data(), 8 * (B + 1)), o_o = put(p->out_off.data(), 8 * (B + 1));
-    size_t o_sc = put(p->scratch_off.data(), 8 * (B + 1));
-    size_t o_n = put(p->nfft.data(), 4 * B);
-    size_t o_it = put(p->items.data(), sizeof(int2) * p->items.size());
-    size_t o_c = put(bank.centre.data(), 8 * bank.centre.size());
-    size_t o_h = put(bank.half.data(), 4 * bank.half.size());
-    size_t o_to = put(bank.tap_off.data(), 8 * bank.tap_off.size());
-    size_t o_tp = put(bank.taps_rev.data(), 8 * bank.taps_rev.size());
-    size_t o_bo = put(p->blk_off.data(), 8 * (B + 1));
-    check(cudaMalloc(&p->meta, blob.size()), "cudaMalloc(plan)");
-    check(cudaMemcpy(p->meta, blob.data(), blob.size(), cudaMemcpyHostToDevice), "cudaMemcpy(plan)");
-    char* m = static_cast<char*>(p->meta);
-    p->d_x_off = reinterpret_cast<int64_t*>(m + o_x);
-    p->d_y_off = reinterpret_cast<int64_t*>(m + o_y);
-    p->d_t_off = reinterpret_cast<int64_t*>(m + o_t);
-    p->d_seg_off = reinterpret_cast<int64_t*>(m + o_s);
-    p->d_frame_off = reinterpret_cast<int64_t*>(m + o_f);
-    p->d_out_off = reinterpret_cast<int64_t*>(m + o_o);
-    p->d_scratch_off = reinterpret_cast<int64_t*>(m + o_sc);
-    p->d_nfft = reinterpret_cast<int*>(m + o_n);
-    p->d_items = reinterpret_cast<int2*>(m + o_it);
-    p->d_centre = reinterpret_cast<double*>(m + o_c);
-    p->d_half = reinterpret_cast<int*>(m + o_h);
-    p->d_tap_off = reinterpret_cast<int64_t*>(m + o_to);
-    p->d_taps = reinterpret_cast<double*>(m + o_tp);
-    p->d_blk_off = reinterpret_cast<int64_t*>(m + o_bo);
-    if (p->use_fft) {
-      if (fft_bank_ctas_per_sm() < 1) throw RuntimeFailure("FFT band-bank kernel does not fit on this device");
-      check(cudaMalloc(&p->filters, sizeof(double2) * (block / 2 + 1) * bank.bands), "cudaMalloc(filters)");
-      check(launch_filter_spectra(p->d_half, p->d_tap_off, p->d_taps, bank.bands, bank.max_half, twiddles,
-                                  p->filters, stream),
-            "filter_spectra");
-      check(cudaStreamSynchronize(stream), "filter_spectra");
-    }
+    p->o_x = put(p->x_off.data(), 8 * (B + 1));
+    p->o_y = put(p->y_off.data(), 8 * (B + 1));
+    p->o_t = put(p->t_off.data(), 8 * (B + 1));
+    p->o_s = put(p->seg_off.data(), 8 * (B + 1));
+    p->o_f = put(p->frame_off.data(), 8 * (B + 1));
+    p->o_o = put(p->out_off.data(), 8 * (B + 1));
+    p->o_sc = put(p->scratch_off.data(), 8 * (B + 1));
+    p->o_n = put(p->nfft.data(), 4 * B);
+    p->o_it = put(p->items.data(), sizeof(int2) * p->items.size());
+    p->o_bo = put(p->blk_off.data(), 8 * (B + 1));
+    if (p->use_fft && fft_bank_ctas_per_sm() < 1)
+      throw RuntimeFailure("FFT band-bank kernel does not fit on this device");
     // Arena layout.
     int per_sm = p->use_fft ? fft_bank_ctas_per_sm() : band_bank_ctas_per_sm(bank.max_pad_taps);
     if (per_sm < 1) throw RuntimeFailure("band-bank kernel does not fit on this device");
@@ -546,6 +630,7 @@ struct Workspace {
     const int64_t F = p->frame_off[B];
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t at = off; off = align_up(off + bytes); return at; };
+    p->at.meta = take(p->meta.size());
     p->at.x = take(8 * p->x_off[B]);
     p->at.u = take(8 * p->t_off[B]);
     p->at.states = take(8 * 3 * p->total_seg);
@@ -869,10 +954,8 @@ void run_host(const double* x, const int64_t* offsets, int clips, const Settings
   WorkspaceCache::Lease lease(cache(), device);
   Workspace& ws = lease.get();
   ContextGuard guard(ws.ctx.get());
-  Plan& p = ws.plan_for(s, offsets, clips);
-  ws.ensure_arena(p.arena_bytes);
+  Plan& p = ws.prepare(s, offsets, clips, ws.stream);
   const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
-  check(cudaStreamWaitEvent(ws.stream, ws.last, 0), "cudaStreamWaitEvent");
   check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyHostToDevice, ws.stream),
         "cudaMemcpy(x)");
   ws.run(p, ws.stream, use_graph, record);
@@ -1040,10 +1123,8 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
     Workspace& ws = lease.get();
     ContextGuard guard(ws.ctx.get());
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ws.stream;
-    Plan& p = ws.plan_for(s, offsets, clips);
-    ws.ensure_arena(p.arena_bytes);
+    Plan& p = ws.prepare(s, offsets, clips, st);
     const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
-    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
     check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyDeviceToDevice, st),
           "cudaMemcpy(x)");
     ws.run(p, st, use_graph, record);
@@ -1073,10 +1154,8 @@ int hv_harvest_grad_forward(const double* x, const int64_t* offsets, int clips, 
     Workspace& ws = lease.get();
     ContextGuard guard(ws.ctx.get());
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
-    Plan& p = ws.plan_for(Settings{fs, f0_floor, f0_ceil, frame_period}, offsets, clips);
-    ws.ensure_arena(p.arena_bytes);
+    Plan& p = ws.prepare(Settings{fs, f0_floor, f0_ceil, frame_period}, offsets, clips, st);
     const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
-    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
     check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyDeviceToDevice, st),
           "cudaMemcpy(x)");
     ws.run(p, st, true, false);
@@ -1101,9 +1180,7 @@ int hv_harvest_grad_backward(const double* x, const int64_t* offsets, int clips,
     Workspace& ws = lease.get();
     ContextGuard guard(ws.ctx.get());
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
-    Plan& p = ws.plan_for(Settings{fs, f0_floor, f0_ceil, frame_period}, offsets, clips);
-    ws.ensure_arena(p.arena_bytes);
-    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
+    Plan& p = ws.prepare(Settings{fs, f0_floor, f0_ceil, frame_period}, offsets, clips, st);
     ws.enqueue_backward(p, x + offsets[0], tape, grad_f0, grad_x + offsets[0], st);
     check(cudaEventRecord(ws.last, st), "cudaEventRecord");
   });
@@ -1121,9 +1198,7 @@ int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor, doubl
     Workspace& ws = lease.get();
     ContextGuard guard(ws.ctx.get());
     int64_t offsets[2] = {0, n};
-    Plan& p = ws.plan_for(Settings{fs, f0_floor, f0_ceil, 5.0}, offsets, 1);
-    ws.ensure_arena(p.arena_bytes);
-    check(cudaStreamWaitEvent(ws.stream, ws.last, 0), "cudaStreamWaitEvent");
+    Plan& p = ws.prepare(Settings{fs, f0_floor, f0_ceil, 5.0}, offsets, 1, ws.stream);
     check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x, 8 * n, cudaMemcpyHostToDevice, ws.stream), "cudaMemcpy(x)");
     ws.run(p, ws.stream, false, false);
     const int64_t F = p.frame_off[1];
