@@ -16,6 +16,7 @@ HV_RUNTIME_ERROR = 2
 HV_DEVICE_POINTERS = 1
 HV_NO_GRAPH = 2
 HV_RECORD_STAGES = 4
+HV_NULL_IS_LEGACY_STREAM = 8
 HV_STAGE_COUNT = 6
 
 _D = ct.POINTER(ct.c_double)
@@ -33,6 +34,9 @@ SIGNATURES = {
     "hv_harvest_batch": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
                                     ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_uint,
                                     ct.c_void_p]),
+    "hv_harvest_batch_pcm16": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                          ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_uint,
+                                          ct.c_void_p]),
     "hv_stage_name": (ct.c_char_p, [ct.c_int]),
     "hv_last_stage_ms": (ct.c_int, [_D]),
     "hv_last_tuning": (ct.c_int, [ct.POINTER(ct.c_int)]),

@@ -23,8 +23,8 @@ import numpy as np
 
 from . import _native
 
-__all__ = ["harvest", "harvest_batch", "harvest_many", "cuda_available", "clear_cache",
-           "output_length", "profile"]
+__all__ = ["harvest", "harvest_batch", "harvest_batch_pcm16", "harvest_many", "cuda_available",
+           "clear_cache", "output_length", "profile"]
 
 _D = ct.POINTER(ct.c_double)
 
@@ -196,6 +196,34 @@ def harvest_batch(x, offsets, fs, f0_floor=71.0, f0_ceil=800.0, frame_period=5.0
     times = np.empty(int(out_off[-1]))
     flags = 0 if graph else _native.HV_NO_GRAPH
     status = _native.lib.hv_harvest_batch(
+        x.ctypes.data, offsets.ctypes.data_as(ct.POINTER(ct.c_int64)), offsets.size - 1, fs,
+        _as_float(f0_floor, "f0_floor"), _as_float(f0_ceil, "f0_ceil"), frame_period, device,
+        f0.ctypes.data, times.ctypes.data, flags, None)
+    _native.raise_for(status)
+    return f0, times, out_off
+
+
+def harvest_batch_pcm16(x, offsets, fs, f0_floor=71.0, f0_ceil=800.0, frame_period=5.0, *, device=0,
+                        graph=True):
+    """``harvest_batch`` on 16-bit PCM samples (a contiguous int16 array,
+    e.g. the frames of a mono PCM16 WAV file). Each sample is taken as
+    sample / 32768, on the device, so the result equals ``harvest_batch`` on
+    ``x / 32768.0`` bit for bit while a quarter of the bytes cross PCIe."""
+    if not isinstance(x, np.ndarray) or x.dtype != np.int16 or x.ndim != 1 or not x.flags.c_contiguous:
+        raise TypeError("x must be a 1-D C-contiguous numpy.ndarray of int16")
+    offsets = np.ascontiguousarray(offsets, dtype=np.int64)
+    if offsets.ndim != 1 or offsets.size < 2:
+        raise ValueError("offsets must hold clips + 1 entries")
+    if offsets[0] < 0 or offsets[-1] > x.size or np.any(np.diff(offsets) < 0):
+        raise ValueError("offsets must be nondecreasing and lie within x")
+    fs = _as_int(fs, "fs")
+    device = _as_int(device, "device")
+    frame_period = _as_float(frame_period, "frame_period")
+    out_off = _out_offsets(offsets, fs, frame_period)
+    f0 = np.empty(int(out_off[-1]))
+    times = np.empty(int(out_off[-1]))
+    flags = 0 if graph else _native.HV_NO_GRAPH
+    status = _native.lib.hv_harvest_batch_pcm16(
         x.ctypes.data, offsets.ctypes.data_as(ct.POINTER(ct.c_int64)), offsets.size - 1, fs,
         _as_float(f0_floor, "f0_floor"), _as_float(f0_ceil, "f0_ceil"), frame_period, device,
         f0.ctypes.data, times.ctypes.data, flags, None)

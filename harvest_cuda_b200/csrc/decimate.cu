@@ -240,6 +240,13 @@ __global__ void flag_nonfinite(const double* __restrict__ x, int64_t total, int*
   if (__syncthreads_or(bad) && threadIdx.x == 0) *flag = 1;
 }
 
+// PCM16 ingestion: sample / 32768, exact in float64 (the conversion of the
+// reference's benchmark for mono PCM16 WAV input, benchmarks/benchmark.py:80-84).
+__global__ void pcm16_to_double(const int16_t* __restrict__ in, int64_t total, double* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = static_cast<double>(in[i]) / 32768.0;
+}
+
 // Ratio 1: the waveform is used as is (harvest.cpp:45-48).
 __global__ void copy_clips(const double* __restrict__ x, int64_t total, double* __restrict__ y) {
   int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -354,6 +361,11 @@ cudaError_t launch_decimate_adjoint(const DecimateView& v, const double* grad_y,
   decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
   adjoint_segment_run<1><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states, grad_x);
   adjoint_edges<<<cgrid, threads, 0, stream>>>(v, states, grad_x);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_pcm16(const int16_t* in, int64_t total, double* out, int sms, cudaStream_t stream) {
+  pcm16_to_double<<<sms * 8, 256, 0, stream>>>(in, total, out);
   return cudaGetLastError();
 }
 

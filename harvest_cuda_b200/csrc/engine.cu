@@ -297,7 +297,7 @@ struct Plan {
   size_t o_x = 0, o_y = 0, o_t = 0, o_s = 0, o_f = 0, o_o = 0, o_sc = 0, o_n = 0, o_it = 0, o_bo = 0;
   size_t arena_bytes = 0;
   struct Layout {
-    size_t meta, x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores,
+    size_t meta, pcm, x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores,
         pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed;
   } at{};
   int bank_ctas = 0;
@@ -631,6 +631,7 @@ struct Workspace {
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t at = off; off = align_up(off + bytes); return at; };
     p->at.meta = take(p->meta.size());
+    p->at.pcm = take(2 * p->x_off[B]);
     p->at.x = take(8 * p->x_off[B]);
     p->at.u = take(8 * p->t_off[B]);
     p->at.states = take(8 * 3 * p->total_seg);
@@ -947,17 +948,26 @@ void collect_stage_ms(Workspace& ws) {
   }
 }
 
-// Shared body of the host-pointer entry points.
+// Shared body of the host-pointer entry points; with `pcm`, the input is
+// PCM16 (x is ignored) and is converted on the device.
 void run_host(const double* x, const int64_t* offsets, int clips, const Settings& s, int device,
-              double* f0, double* times, bool use_graph, bool record) {
+              double* f0, double* times, bool use_graph, bool record, const int16_t* pcm = nullptr) {
   check_device(device);
   WorkspaceCache::Lease lease(cache(), device);
   Workspace& ws = lease.get();
   ContextGuard guard(ws.ctx.get());
   Plan& p = ws.prepare(s, offsets, clips, ws.stream);
   const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
-  check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyHostToDevice, ws.stream),
-        "cudaMemcpy(x)");
+  if (pcm) {
+    check(cudaMemcpyAsync(ws.ptr<int16_t>(p.at.pcm), pcm + offsets[0], 2 * total_x, cudaMemcpyHostToDevice,
+                          ws.stream),
+          "cudaMemcpy(pcm)");
+    check(launch_pcm16(ws.ptr<int16_t>(p.at.pcm), total_x, ws.ptr<double>(p.at.x), ws.sms, ws.stream), "pcm16");
+  } else {
+    check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyHostToDevice,
+                          ws.stream),
+          "cudaMemcpy(x)");
+  }
   ws.run(p, ws.stream, use_graph, record);
   // Samples are checked for finiteness on the device; nothing is copied back
   // for input the reference would have rejected.
@@ -1122,7 +1132,8 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
     WorkspaceCache::Lease lease(cache(), device);
     Workspace& ws = lease.get();
     ContextGuard guard(ws.ctx.get());
-    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : ws.stream;
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream)
+                             : ((flags & HV_NULL_IS_LEGACY_STREAM) ? cudaStreamLegacy : ws.stream);
     Plan& p = ws.prepare(s, offsets, clips, st);
     const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
     check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * total_x, cudaMemcpyDeviceToDevice, st),
@@ -1140,6 +1151,37 @@ int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
       check(cudaStreamSynchronize(st), "harvest_batch");
       collect_stage_ms(ws);
     }
+  });
+}
+
+int hv_harvest_batch_pcm16(const int16_t* x, const int64_t* offsets, int clips, int fs, double f0_floor,
+                           double f0_ceil, double frame_period, int device, double* f0, double* times,
+                           unsigned flags, void* stream) {
+  return guarded([&] {
+    validate_batch(offsets, clips, fs, f0_floor, f0_ceil, frame_period);
+    if (!x || !f0) throw InvalidArgument("null buffer");
+    Settings s{fs, f0_floor, f0_ceil, frame_period};
+    const bool use_graph = !(flags & HV_NO_GRAPH);
+    if (!(flags & HV_DEVICE_POINTERS)) {
+      run_host(nullptr, offsets, clips, s, device, f0, times, use_graph, false, x);
+      return;
+    }
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream)
+                             : ((flags & HV_NULL_IS_LEGACY_STREAM) ? cudaStreamLegacy : ws.stream);
+    Plan& p = ws.prepare(s, offsets, clips, st);
+    const int64_t total_x = p.x_off[clips], total_out = p.out_off[clips];
+    check(launch_pcm16(x + offsets[0], total_x, ws.ptr<double>(p.at.x), ws.sms, st), "pcm16");
+    ws.run(p, st, use_graph, false);
+    check(cudaMemcpyAsync(f0, ws.ptr<double>(p.at.f0), 8 * total_out, cudaMemcpyDeviceToDevice, st),
+          "cudaMemcpy(f0)");
+    if (times)
+      check(cudaMemcpyAsync(times, ws.ptr<double>(p.at.times), 8 * total_out, cudaMemcpyDeviceToDevice, st),
+            "cudaMemcpy(times)");
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
   });
 }
 

@@ -39,6 +39,9 @@ extern "C" {
 #define HV_RECORD_STAGES 4u   /* launch stage by stage with CUDA events between stages; the
                                  call waits for the GPU and hv_last_stage_ms() returns the
                                  per-stage device milliseconds of this call */
+#define HV_NULL_IS_LEGACY_STREAM 8u /* with HV_DEVICE_POINTERS: a NULL `stream` is the legacy
+                                 default stream (PyTorch's default stream), not the
+                                 engine's own */
 
 /* Message describing the last failure on the calling thread ("" if none). */
 HV_API const char* hv_last_error(void);
@@ -78,6 +81,17 @@ HV_API int hv_harvest(const double* x, int64_t n, int fs, double f0_floor, doubl
 HV_API int hv_harvest_batch(const double* x, const int64_t* offsets, int clips, int fs,
                      double f0_floor, double f0_ceil, double frame_period, int device,
                      double* f0, double* times, unsigned flags, void* stream);
+
+/* hv_harvest_batch on 16-bit PCM input: each sample is read as
+ * sample / 32768, the conversion the reference's benchmark applies to mono
+ * PCM16 WAV files (reference benchmarks/benchmark.py:80-84), so results equal
+ * hv_harvest_batch on the converted samples bit for bit. The conversion runs
+ * on the device, so a host batch crosses PCIe at 2 bytes per sample instead
+ * of 8. Flags as hv_harvest_batch (HV_RECORD_STAGES excepted). No counterpart
+ * in the reference's API. */
+HV_API int hv_harvest_batch_pcm16(const int16_t* x, const int64_t* offsets, int clips, int fs,
+                                  double f0_floor, double f0_ceil, double frame_period, int device,
+                                  double* f0, double* times, unsigned flags, void* stream);
 
 /* Like hv_harvest, also reporting per-stage device milliseconds into
  * stage_ms[HV_STAGE_COUNT] (reference _profile, src/bindings.cpp:90-104). */
