@@ -37,6 +37,8 @@ SIGNATURES = {
     "hv_harvest_batch_pcm16": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
                                           ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_uint,
                                           ct.c_void_p]),
+    "hv_compare_batch": (ct.c_int, [ct.c_void_p, ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_void_p, ct.c_uint,
+                                    ct.c_void_p]),
     "hv_stage_name": (ct.c_char_p, [ct.c_int]),
     "hv_last_stage_ms": (ct.c_int, [_D]),
     "hv_last_tuning": (ct.c_int, [ct.POINTER(ct.c_int)]),

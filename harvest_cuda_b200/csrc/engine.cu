@@ -371,6 +371,8 @@ struct Workspace {
   std::map<Settings, std::unique_ptr<DeviceBank>> device_banks;
   uint64_t next_plan_id = 1;
   uint64_t meta_owner = 0;   // plan whose tables are at the head of the arena
+  void* metric_buf = nullptr;   // inputs and offsets of hv_compare_batch
+  size_t metric_size = 0;
 
   explicit Workspace(int dev) : device(dev), ctx(dev) {
     ContextGuard g(ctx.get());
@@ -391,6 +393,7 @@ struct Workspace {
       plans.clear();
       device_banks.clear();
       if (arena) cudaFree(arena);
+      if (metric_buf) cudaFree(metric_buf);
       if (twiddles) cudaFree(twiddles);
       if (host_flag) cudaFreeHost(host_flag);
       for (auto& e : marks) if (e) cudaEventDestroy(e);
@@ -1181,6 +1184,63 @@ int hv_harvest_batch_pcm16(const int16_t* x, const int64_t* offsets, int clips, 
     if (times)
       check(cudaMemcpyAsync(times, ws.ptr<double>(p.at.times), 8 * total_out, cudaMemcpyDeviceToDevice, st),
             "cudaMemcpy(times)");
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
+  });
+}
+
+int hv_compare_batch(const double* reference, const double* f0, const int64_t* offsets, int clips, int device,
+                     double* stats, unsigned flags, void* stream) {
+  return guarded([&] {
+    if (clips <= 0 || !offsets) throw InvalidArgument("a batch needs at least one clip and its offsets");
+    if (!reference || !f0 || !stats) throw InvalidArgument("null buffer");
+    if (offsets[0] < 0) throw InvalidArgument("offsets must be nonnegative");
+    for (int c = 0; c < clips; ++c)
+      if (offsets[c + 1] < offsets[c]) throw InvalidArgument("offsets must be nondecreasing");
+    const int64_t base = offsets[0], total = offsets[clips] - offsets[0];
+    const bool on_device = (flags & HV_DEVICE_POINTERS) != 0;
+    if (!on_device)
+      for (int64_t i = base; i < base + total; ++i)
+        if (!std::isfinite(reference[i]) || !std::isfinite(f0[i]) || reference[i] < 0 || f0[i] < 0)
+          throw InvalidArgument("F0 tracks must contain only finite, nonnegative values");
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = ws.stream;
+    if (on_device && stream) st = static_cast<cudaStream_t>(stream);
+    else if (on_device && (flags & HV_NULL_IS_LEGACY_STREAM)) st = cudaStreamLegacy;
+    // Workspace buffer: [relative offsets | reference | f0 | stats]; the
+    // tracks and stats only for host inputs.
+    const size_t off_bytes = align_up(8 * size_t(clips + 1));
+    const size_t track_bytes = on_device ? 0 : align_up(8 * size_t(total));
+    const size_t stat_bytes = on_device ? 0 : align_up(8 * 7 * size_t(clips));
+    const size_t need = off_bytes + 2 * track_bytes + stat_bytes;
+    if (need > ws.metric_size) {
+      check(cudaEventSynchronize(ws.last), "cudaEventSynchronize");
+      if (ws.metric_buf) cudaFree(ws.metric_buf);
+      ws.metric_buf = nullptr;
+      ws.metric_size = 0;
+      check(cudaMalloc(&ws.metric_buf, need), "cudaMalloc(metrics)");
+      ws.metric_size = need;
+    }
+    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
+    char* m = static_cast<char*>(ws.metric_buf);
+    std::vector<int64_t> rel(clips + 1);
+    for (int c = 0; c <= clips; ++c) rel[c] = offsets[c] - base;
+    int64_t* d_off = reinterpret_cast<int64_t*>(m);
+    check(cudaMemcpyAsync(d_off, rel.data(), 8 * rel.size(), cudaMemcpyHostToDevice, st), "cudaMemcpy(offsets)");
+    if (on_device) {
+      check(launch_compare(reference + base, f0 + base, d_off, clips, stats, st), "compare");
+    } else {
+      double* d_ref = reinterpret_cast<double*>(m + off_bytes);
+      double* d_f0 = reinterpret_cast<double*>(m + off_bytes + track_bytes);
+      double* d_stats = reinterpret_cast<double*>(m + off_bytes + 2 * track_bytes);
+      check(cudaMemcpyAsync(d_ref, reference + base, 8 * total, cudaMemcpyHostToDevice, st), "cudaMemcpy(reference)");
+      check(cudaMemcpyAsync(d_f0, f0 + base, 8 * total, cudaMemcpyHostToDevice, st), "cudaMemcpy(f0)");
+      check(launch_compare(d_ref, d_f0, d_off, clips, d_stats, st), "compare");
+      check(cudaMemcpyAsync(stats, d_stats, 8 * 7 * size_t(clips), cudaMemcpyDeviceToHost, st), "cudaMemcpy(stats)");
+      check(cudaStreamSynchronize(st), "compare");
+    }
     check(cudaEventRecord(ws.last, st), "cudaEventRecord");
   });
 }

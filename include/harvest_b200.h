@@ -115,6 +115,22 @@ HV_API int hv_profile(const double* x, int64_t n, int fs, double f0_floor, doubl
  * off (shape 4, 32). */
 HV_API int hv_last_tuning(int* shape);
 
+/* Accuracy of one F0 track against another for every clip of a batch,
+ * computed on the device: the statistics of the reference's benchmark
+ * comparison (reference benchmarks/benchmark.py:20-37). reference and f0 are
+ * packed alike, clip c spanning [offsets[c], offsets[c+1]) (offsets: host,
+ * clips + 1 entries). stats receives 7 doubles per clip: frames,
+ * reference-voiced frames, jointly voiced frames, voiced/unvoiced
+ * disagreement (fraction of frames), 99th-percentile and maximum
+ * |1200 log2(f0 / reference)| cents over jointly voiced frames (numpy's
+ * linear quantile; NaN without such frames), and the count above 600 cents.
+ * With HV_DEVICE_POINTERS the tracks and stats are device memory and the call
+ * is ordered on `stream` (HV_NULL_IS_LEGACY_STREAM as for hv_harvest_batch);
+ * otherwise host memory, validated as finite and nonnegative, and the call
+ * returns with the stats. No counterpart in the reference's API. */
+HV_API int hv_compare_batch(const double* reference, const double* f0, const int64_t* offsets, int clips,
+                            int device, double* stats, unsigned flags, void* stream);
+
 /* F0 gradient (no reference counterpart; the reference has no derivative).
  * Harvest is piecewise smooth in x: with every discrete choice of a forward
  * pass held fixed (candidates kept, voicing, FixF0Contour's choices, the
