@@ -205,8 +205,8 @@ def _world_clip(args):
     import oracle
     checker = oracle.best()
     t0 = time.perf_counter()
-    checker.harvest(x, fs, floor, ceil, period)
-    return time.perf_counter() - t0, checker.name
+    f0, _ = checker.harvest(x, fs, floor, ceil, period)
+    return time.perf_counter() - t0, checker.name, f0
 
 
 def cpu_sample(wl, target_seconds, cores):
@@ -233,7 +233,31 @@ def run_cpu(pool, wl, clips):
     wall = time.perf_counter() - t0
     audio = sum(t[0].size for t in tasks) / wl["fs"]
     kind = "reference" if results and results[0][1] == "reference" else "port"
+    run_cpu.last_f0 = [r[2] for r in results]
     return audio, wall, kind
+
+
+def accuracy_against(reference_f0, sample, f0, out_off, kind, device):
+    """The engine's batch output (the last end-to-end step) against the CPU
+    reference's F0 for the sampled clips, compared per clip on the device
+    (metrics.compare_batch) and summarised over the sample."""
+    from harvest_cuda_b200.metrics import compare_batch
+    ours = np.concatenate([f0[out_off[i]:out_off[i + 1]] for i in sample])
+    ref = np.concatenate(reference_f0)
+    offsets = np.concatenate([[0], np.cumsum([len(r) for r in reference_f0])])
+    stats = compare_batch(ref, ours, offsets, device=device)
+    frames = sum(s["frames"] for s in stats)
+    both = (ref > 0) & (ours > 0)
+    rel = np.abs(ours[both] - ref[both]) / ref[both]
+    p99 = [s["cents_p99"] for s in stats if s["cents_p99"] is not None]
+    cmax = [s["cents_max"] for s in stats if s["cents_max"] is not None]
+    return {"against": "WORLD Harvest (oracle/_ref)" if kind == "reference" else "C restatement (oracle)",
+            "clips": len(stats), "frames": frames,
+            "vuv_disagreement": sum(s["vuv_disagreement"] * s["frames"] for s in stats) / max(frames, 1),
+            "cents_p99_max_over_clips": max(p99) if p99 else None, "cents_max": max(cmax) if cmax else None,
+            "over_600_cents": sum(s["over_600_cents"] for s in stats),
+            "voiced_f0_rel_max": float(rel.max()) if rel.size else None,
+            "computed_on": "device, hv_compare_batch (rel_max on the host)"}
 
 
 def kernels_per_step(ratio):
@@ -466,6 +490,7 @@ def run_ours(args):
                 "value": a / wall, "unit": "audio-s/s", "cores": cores, "kind": kind,
                 "sample": f"{len(sample)} of the batch's clips ({a:.1f} audio-s), one clip per "
                           f"worker process, {wall:.1f} s wall"}
+            line["accuracy"] = accuracy_against(run_cpu.last_f0, sample, f0, out_off, kind, local)
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()
