@@ -179,8 +179,8 @@ band_bank_fir(BankView v, const double* __restrict__ y, const double* __restrict
 
     // Interpolate the four interval tracks at every 1 ms frame.
     const int64_t f_begin = B.frame_off[c];
-    band_contour(B, ev, count, v.centre[b], raw + b * v.total_frames + f_begin,
-                 static_cast<int>(B.frame_off[c + 1] - f_begin));
+    band_contour_walk(B, ev, count, v.centre[b], raw + b * v.total_frames + f_begin,
+                      static_cast<int>(B.frame_off[c + 1] - f_begin));
   }
 }
 

@@ -93,7 +93,6 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
   __shared__ int item_slot;
   __shared__ double red[3 * (kFftThreads / 32)];
   __shared__ unsigned long long scan_scratch[kFftThreads / 32];
-  __shared__ int chunk_bounds[8 * kFftThreads];
   const BatchView& B = v.batch;
   const int tid = threadIdx.x;
   double* xs = reinterpret_cast<double*>(buf);
@@ -168,51 +167,53 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
       // (i < run) and the two lookahead samples one slot further.
       const double* mine_lin = xs + q_lo + min(tid, edge_end / run + 1);
       auto X = [&](int i) -> double { return mine_lin[i + (i >= run ? 1 : 0)]; };
-      const int len = q_hi - q_lo;
-      unsigned long long mine = 0;
+      const int len = q_hi - q_lo;   // run <= 32: hits fit one bit mask per kind
+      unsigned hits[4] = {0u, 0u, 0u, 0u};
       for (int i0 = 0; i0 < len; i0 += 8) {
         double v[10];
 #pragma unroll
         for (int u = 0; u < 10; ++u) v[u] = X(i0 + u);
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-          const int q = q_lo + i0 + u;
-          if (i0 + u >= len) break;
+          const int i = i0 + u;
+          if (i >= len) break;
           const double f0 = v[u], f1 = v[u + 1], f2 = v[u + 2];
           const double a0 = -f0, a1 = -f1, a2 = -f2;
           const double d0 = a0 - a1, d1 = a1 - a2;
-          mine += (0.0 < f0 && f1 <= 0.0) ? 1ull : 0ull;
-          mine += (0.0 < a0 && a1 <= 0.0) ? (1ull << 16) : 0ull;
-          if (q < peak_end) {
-            mine += (0.0 < d0 && d1 <= 0.0) ? (1ull << 32) : 0ull;
-            mine += (0.0 < -d0 && -d1 <= 0.0) ? (1ull << 48) : 0ull;
+          hits[0] |= (0.0 < f0 && f1 <= 0.0) ? 1u << i : 0u;
+          hits[1] |= (0.0 < a0 && a1 <= 0.0) ? 1u << i : 0u;
+          if (q_lo + i < peak_end) {
+            hits[2] |= (0.0 < d0 && d1 <= 0.0) ? 1u << i : 0u;
+            hits[3] |= (0.0 < -d0 && -d1 <= 0.0) ? 1u << i : 0u;
           }
         }
       }
+      const unsigned long long mine = static_cast<unsigned long long>(__popc(hits[0])) |
+                                      static_cast<unsigned long long>(__popc(hits[1])) << 16 |
+                                      static_cast<unsigned long long>(__popc(hits[2])) << 32 |
+                                      static_cast<unsigned long long>(__popc(hits[3])) << 48;
       unsigned long long total;
       const unsigned long long before = block_scan_packed(mine, scan_scratch, total);
-      int at[4];
+      // Second pass over the hits only: a warp runs each kind's loop as many
+      // times as its busiest lane has hits, so the division of every edge is
+      // issued once per hit rather than once per sample any lane hits.
 #pragma unroll
-      for (int k = 0; k < 4; ++k) at[k] = count[k] + static_cast<int>((before >> (16 * k)) & 0xffff);
-      for (int i0 = 0; i0 < len; i0 += 8) {
-        double v[10];
-#pragma unroll
-        for (int u = 0; u < 10; ++u) v[u] = X(i0 + u);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int q = q_lo + i0 + u;
-          if (i0 + u >= len) break;
-          const double f0 = v[u], f1 = v[u + 1], f2 = v[u + 2];
-          const int64_t e = o + q + 1;
-          const double a0 = -f0, a1 = -f1, a2 = -f2;
-          const double d0 = a0 - a1, d1 = a1 - a2;
-          if (0.0 < f0 && f1 <= 0.0) ev[0][at[0]++] = fine_edge(e, f0, f1);
-          if (0.0 < a0 && a1 <= 0.0) ev[1][at[1]++] = fine_edge(e, a0, a1);
-          if (q < peak_end) {
-            if (0.0 < d0 && d1 <= 0.0) ev[2][at[2]++] = fine_edge(e, d0, d1);
-            const double e0 = -d0, e1 = -d1;
-            if (0.0 < e0 && e1 <= 0.0) ev[3][at[3]++] = fine_edge(e, e0, e1);
+      for (int k = 0; k < 4; ++k) {
+        double* dst = ev[k] + count[k] + static_cast<int>((before >> (16 * k)) & 0xffff);
+        for (unsigned m = hits[k]; m; m &= m - 1) {
+          const int i = __ffs(m) - 1;
+          const double f0 = X(i), f1 = X(i + 1);
+          double s0, s1;
+          if (k < 2) {
+            s0 = k == 0 ? f0 : -f0;
+            s1 = k == 0 ? f1 : -f1;
+          } else {
+            const double a0 = -f0, a1 = -f1, a2 = -X(i + 2);
+            const double d0 = a0 - a1, d1 = a1 - a2;
+            s0 = k == 2 ? d0 : -d0;
+            s1 = k == 2 ? d1 : -d1;
           }
+          *dst++ = fine_edge(o + q_lo + i + 1, s0, s1);
         }
       }
 #pragma unroll
@@ -220,8 +221,8 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
     }
     __syncthreads();
     const int64_t f_begin = B.frame_off[c];
-    band_contour_staged(B, ev, count, v.centre[b], raw + b * v.total_frames + f_begin,
-                        static_cast<int>(B.frame_off[c + 1] - f_begin), chunk_bounds, xs, 2 * kFftPadded);
+    band_contour_walk(B, ev, count, v.centre[b], raw + b * v.total_frames + f_begin,
+                      static_cast<int>(B.frame_off[c + 1] - f_begin));
   }
 }
 

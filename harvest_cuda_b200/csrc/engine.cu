@@ -729,6 +729,8 @@ struct Workspace {
     check(cudaMemsetAsync(ptr<int>(p.at.queue), 0, 16, s), "memset");
     if (p.use_fft) {
       const int run = 2 * ((p.fft_valid + 2 + 2 * 256 - 1) / (2 * 256));
+      // The event scan keeps one 32-bit hit mask per kind and thread run.
+      if (run > 32) throw RuntimeFailure("FFT band bank: event run longer than 32 positions");
       FftBankGeometry geo{p.bank->max_half, p.fft_valid, run, p.total_blocks, p.d_blk_off};
       check(launch_fft_bank(kv, geo, y, ptr<double>(p.at.bins), twiddles, p.filters, ptr<double2>(p.at.spectra),
                             ptr<int>(p.at.queue), ptr<double>(p.at.slots), p.bank_ctas, ptr<double>(p.at.raw), s),

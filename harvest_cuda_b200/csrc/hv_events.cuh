@@ -86,47 +86,11 @@ __device__ __forceinline__ double fine_edge(int64_t e, double s0, double s1) {
 }
 
 // interp1 with histc clamping (matlabfunctions.cpp:136-176) of the
-// interval track derived from `count` fine edges (harvest.cpp:188-191):
-// locations (e_j + e_{j+1}) / 2 / fs, values fs / (e_{j+1} - e_j).
-__device__ inline double interval_at(const double* edges, int count, double fs, double t) {
-  const int intervals = count - 1;
-  int lo = 0, hi = intervals;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    const double loc = (edges[mid] + edges[mid + 1]) / 2.0 / fs;
-    if (loc <= t) lo = mid + 1; else hi = mid;
-  }
-  const int seg = imin(imax(lo, 1), intervals - 1);
-  const double x0 = (edges[seg - 1] + edges[seg]) / 2.0 / fs;
-  const double x1 = (edges[seg] + edges[seg + 1]) / 2.0 / fs;
-  const double y0 = fs / (edges[seg] - edges[seg - 1]);
-  const double y1 = fs / (edges[seg + 1] - edges[seg]);
-  const double s = (t - x0) / (x1 - x0);
-  return y0 + s * (y1 - y0);
-}
-
-// GetF0CandidateContour(Sub) (harvest.cpp:240-293) for one band of one
-// clip: the mean of the four interpolated tracks at t = frame / 1000,
-// limited to [0.9, 1.1] x centre and [floor, ceil]; all zero unless every
-// track has more than two intervals.
-__device__ inline void band_contour(const BatchView& B, double* const ev[4], const int count[4],
-                                    double centre, double* out, int frames) {
-  const bool usable = count[0] - 1 > 2 && count[1] - 1 > 2 && count[2] - 1 > 2 && count[3] - 1 > 2;
-  const double upper = centre * 1.1, lower = centre * 0.9;
-  for (int f = threadIdx.x; f < frames; f += blockDim.x) {
-    double val = 0.0;
-    if (usable) {
-      const double t = f * 1 / 1000.0;
-      const double i0 = interval_at(ev[0], count[0], B.fs_r, t);
-      const double i1 = interval_at(ev[1], count[1], B.fs_r, t);
-      const double i2 = interval_at(ev[2], count[2], B.fs_r, t);
-      const double i3 = interval_at(ev[3], count[3], B.fs_r, t);
-      val = (i0 + i1 + i2 + i3) / 4.0;
-      if (val > upper || val < lower || val > B.f0_ceil || val < B.f0_floor) val = 0.0;
-    }
-    out[f] = val;
-  }
-}
+// interval tracks derived from the fine edges (harvest.cpp:188-191):
+// locations (e_j + e_{j+1}) / 2 / fs, values fs / (e_{j+1} - e_j), and
+// GetF0CandidateContour(Sub) (harvest.cpp:240-293): the mean of the four
+// interpolated tracks at t = frame / 1000, limited to [0.9, 1.1] x centre and
+// [floor, ceil]; all zero unless every track has more than two intervals.
 
 // Interval segment used at time t (histc clamping): the number of interval
 // locations <= t, clamped to [1, intervals - 1]; by binary search over the
@@ -141,119 +105,57 @@ __device__ inline int segment_at(const double* edges, int count, double fs, doub
   return imin(imax(lo, 1), intervals - 1);
 }
 
-// band_contour for one CTA, with the event lists staged through shared
-// memory: frames go in chunks of blockDim.x; the segments a chunk can use
-// lie between the segments of its first and last frame, so that slice of
-// every list is copied to `stage` (coalesced) and searched there. Chunk
-// bounds are found for up to blockDim.x chunks at once, one thread each.
-// `bounds` holds 8 * blockDim.x ints; `stage` holds `capacity` doubles.
-// A chunk whose slices do not fit falls back to searches in global memory.
-__device__ inline void band_contour_staged(const BatchView& B, double* const ev[4], const int count[4],
-                                           double centre, double* out, int frames, int* bounds,
-                                           double* stage, int capacity) {
+// band_contour for one CTA, each thread walking a contiguous run of frames.
+// Frame times only increase, so after one binary search for the run's first
+// frame (segment_at) the histc segment of every later frame is found by
+// stepping forward while the next interval location is <= t; each interval
+// location and value is computed once, with the reference's expressions, as
+// the walk passes it. The results equal interval_at's bit for bit.
+__device__ inline void band_contour_walk(const BatchView& B, double* const ev[4], const int count[4],
+                                         double centre, double* out, int frames) {
   const int nt = blockDim.x, tid = threadIdx.x;
+  const int per = (frames + nt - 1) / nt;
+  const int fa = imin(tid * per, frames), fb = imin(fa + per, frames);
   const bool usable = count[0] - 1 > 2 && count[1] - 1 > 2 && count[2] - 1 > 2 && count[3] - 1 > 2;
   if (!usable) {
-    for (int f = tid; f < frames; f += nt) out[f] = 0.0;
+    for (int f = fa; f < fb; ++f) out[f] = 0.0;
     return;
   }
+  if (fa >= fb) return;
   const double fs = B.fs_r;
   const double upper = centre * 1.1, lower = centre * 0.9;
-  const int chunks = (frames + nt - 1) / nt;
-  for (int g0 = 0; g0 < chunks; g0 += nt) {
-    const int group = imin(nt, chunks - g0);
-    __syncthreads();
-    // 8 searches per chunk (first and last frame, four tracks), one per
-    // thread, so their dependent loads overlap instead of queueing.
-    for (int w = tid; w < 8 * group; w += nt) {
-      const int ci = w >> 3, which = w & 7, k = which >> 1;
-      const int first = (g0 + ci) * nt;
-      const int frame = (which & 1) ? imin(first + nt, frames) - 1 : first;
-      bounds[which * nt + ci] = segment_at(ev[k], count[k], fs, frame * 1 / 1000.0);
-    }
-    __syncthreads();
-    for (int ci = 0; ci < group; ++ci) {
-      // Intervals lo-1 .. hi of each track: their locations and values,
-      // computed once per chunk exactly as the reference writes them
-      // (harvest.cpp:188-191).
-      int lo[4], hi[4], base[4], total = 0;
-      for (int k = 0; k < 4; ++k) {
-        lo[k] = bounds[(2 * k) * nt + ci];
-        hi[k] = bounds[(2 * k + 1) * nt + ci];
-        base[k] = total;
-        total += 2 * (hi[k] - lo[k] + 2);
+  int seg[4], last[4];
+  double x0[4], x1[4], y0[4], y1[4];
+  const double t0 = fa * 1 / 1000.0;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double* e = ev[k];
+    last[k] = count[k] - 2;                       // intervals - 1
+    seg[k] = segment_at(e, count[k], fs, t0);
+    const int j = seg[k];
+    x0[k] = (e[j - 1] + e[j]) / 2.0 / fs;
+    x1[k] = (e[j] + e[j + 1]) / 2.0 / fs;
+    y0[k] = fs / (e[j] - e[j - 1]);
+    y1[k] = fs / (e[j + 1] - e[j]);
+  }
+  for (int f = fa; f < fb; ++f) {
+    const double t = f * 1 / 1000.0;
+    double track[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      while (seg[k] < last[k] && x1[k] <= t) {
+        const double* e = ev[k] + (++seg[k]);
+        x0[k] = x1[k];
+        y0[k] = y1[k];
+        x1[k] = (e[0] + e[1]) / 2.0 / fs;
+        y1[k] = fs / (e[1] - e[0]);
       }
-      const bool staged = total <= capacity;
-      __syncthreads();
-      if (staged)
-        for (int k = 0; k < 4; ++k) {
-          const int n_int = hi[k] - lo[k] + 2;
-          double* loc = stage + base[k];
-          double* val = loc + n_int;
-          for (int i = tid; i < n_int; i += nt) {
-            const double a = ev[k][lo[k] - 1 + i], b = ev[k][lo[k] + i];
-            loc[i] = (a + b) / 2.0 / fs;
-            val[i] = fs / (b - a);
-          }
-        }
-      __syncthreads();
-      const int f = (g0 + ci) * nt + tid;
-      if (f >= frames) continue;
-      const double t = f * 1 / 1000.0;
-      double track[4];
-      if (staged) {
-        // The four searches are independent; unrolled they overlap.
-        int a[4], b[4];
-        const double* loc[4];
-        const double* val[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int n_int = hi[k] - lo[k] + 2;
-          loc[k] = stage + base[k] - (lo[k] - 1);   // loc[j], j in [lo-1, hi]
-          val[k] = loc[k] + n_int;
-          a[k] = lo[k];
-          b[k] = hi[k];
-        }
-        // seg = lo + #{j in [lo, hi) : loc[j] <= t}
-        bool more = true;
-        while (more) {
-          more = false;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            if (a[k] < b[k]) {
-              const int mid = (a[k] + b[k]) >> 1;
-              if (loc[k][mid] <= t) a[k] = mid + 1; else b[k] = mid;
-              more |= a[k] < b[k];
-            }
-          }
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const double x0 = loc[k][a[k] - 1], x1 = loc[k][a[k]];
-          const double y0 = val[k][a[k] - 1], y1 = val[k][a[k]];
-          const double s = (t - x0) / (x1 - x0);
-          track[k] = y0 + s * (y1 - y0);
-        }
-      } else {
-        for (int k = 0; k < 4; ++k) {
-          const double* e = ev[k];
-          int a = lo[k], b = hi[k];
-          while (a < b) {
-            const int mid = (a + b) >> 1;
-            if ((e[mid] + e[mid + 1]) / 2.0 / fs <= t) a = mid + 1; else b = mid;
-          }
-          const double x0 = (e[a - 1] + e[a]) / 2.0 / fs;
-          const double x1 = (e[a] + e[a + 1]) / 2.0 / fs;
-          const double y0 = fs / (e[a] - e[a - 1]);
-          const double y1 = fs / (e[a + 1] - e[a]);
-          const double s = (t - x0) / (x1 - x0);
-          track[k] = y0 + s * (y1 - y0);
-        }
-      }
-      double val = (track[0] + track[1] + track[2] + track[3]) / 4.0;
-      if (val > upper || val < lower || val > B.f0_ceil || val < B.f0_floor) val = 0.0;
-      out[f] = val;
+      const double s = (t - x0[k]) / (x1[k] - x0[k]);
+      track[k] = y0[k] + s * (y1[k] - y0[k]);
     }
+    double val = (track[0] + track[1] + track[2] + track[3]) / 4.0;
+    if (val > upper || val < lower || val > B.f0_ceil || val < B.f0_floor) val = 0.0;
+    out[f] = val;
   }
 }
 
