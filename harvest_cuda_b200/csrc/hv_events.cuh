@@ -92,25 +92,16 @@ __device__ __forceinline__ double fine_edge(int64_t e, double s0, double s1) {
 // interpolated tracks at t = frame / 1000, limited to [0.9, 1.1] x centre and
 // [floor, ceil]; all zero unless every track has more than two intervals.
 
-// Interval segment used at time t (histc clamping): the number of interval
-// locations <= t, clamped to [1, intervals - 1]; by binary search over the
-// fine edges in global memory.
-__device__ inline int segment_at(const double* edges, int count, double fs, double t) {
-  const int intervals = count - 1;
-  int lo = 0, hi = intervals;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if ((edges[mid] + edges[mid + 1]) / 2.0 / fs <= t) lo = mid + 1; else hi = mid;
-  }
-  return imin(imax(lo, 1), intervals - 1);
-}
-
 // band_contour for one CTA, each thread walking a contiguous run of frames.
-// Frame times only increase, so after one binary search for the run's first
-// frame (segment_at) the histc segment of every later frame is found by
-// stepping forward while the next interval location is <= t; each interval
-// location and value is computed once, with the reference's expressions, as
-// the walk passes it. The results equal interval_at's bit for bit.
+// The histc segment of a time t is the number of interval locations <= t,
+// clamped to [1, intervals - 1]. A binary search finds it for the run's
+// first frame; frame times only increase, so for every later frame it is
+// found by stepping forward while the next interval location is <= t. The four
+// tracks step in lockstep (one iteration advances every track that needs it)
+// so that their loads and divisions overlap; each track keeps the two edges
+// of its current right interval, so a step loads one edge. Every interval
+// location and value is computed with the reference's expressions, so the
+// results equal a binary search per frame bit for bit.
 __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4], const int count[4],
                                          double centre, double* out, int frames) {
   const int nt = blockDim.x, tid = threadIdx.x;
@@ -125,31 +116,68 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
   const double fs = B.fs_r;
   const double upper = centre * 1.1, lower = centre * 0.9;
   int seg[4], last[4];
-  double x0[4], x1[4], y0[4], y1[4];
+  double x0[4], x1[4], y0[4], y1[4], ea[4], eb[4];   // ea, eb: edges seg, seg + 1
   const double t0 = fa * 1 / 1000.0;
+  // The first frame's segment of the four tracks, by binary searches
+  // interleaved so that their dependent loads overlap.
+  int lo[4], hi[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    last[k] = count[k] - 2;                       // intervals - 1
+    lo[k] = 0;
+    hi[k] = count[k] - 1;
+  }
+  for (bool more = true; more;) {
+    more = false;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      if (lo[k] >= hi[k]) continue;
+      const int mid = (lo[k] + hi[k]) >> 1;
+      if ((ev[k][mid] + ev[k][mid + 1]) / 2.0 / fs <= t0) lo[k] = mid + 1; else hi[k] = mid;
+      more |= lo[k] < hi[k];
+    }
+  }
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const double* e = ev[k];
-    last[k] = count[k] - 2;                       // intervals - 1
-    seg[k] = segment_at(e, count[k], fs, t0);
+    seg[k] = imin(imax(lo[k], 1), last[k]);
     const int j = seg[k];
-    x0[k] = (e[j - 1] + e[j]) / 2.0 / fs;
-    x1[k] = (e[j] + e[j + 1]) / 2.0 / fs;
-    y0[k] = fs / (e[j] - e[j - 1]);
-    y1[k] = fs / (e[j + 1] - e[j]);
+    const double em = e[j - 1];
+    ea[k] = e[j];
+    eb[k] = e[j + 1];
+    x0[k] = (em + ea[k]) / 2.0 / fs;
+    x1[k] = (ea[k] + eb[k]) / 2.0 / fs;
+    y0[k] = fs / (ea[k] - em);
+    y1[k] = fs / (eb[k] - ea[k]);
   }
   for (int f = fa; f < fb; ++f) {
     const double t = f * 1 / 1000.0;
+    for (;;) {
+      bool step[4], any = false;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        step[k] = seg[k] < last[k] && x1[k] <= t;
+        any |= step[k];
+      }
+      if (!any) break;
+      double next[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) next[k] = step[k] ? ev[k][seg[k] + 2] : 0.0;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (!step[k]) continue;
+        ++seg[k];
+        x0[k] = x1[k];
+        y0[k] = y1[k];
+        ea[k] = eb[k];
+        eb[k] = next[k];
+        x1[k] = (ea[k] + eb[k]) / 2.0 / fs;
+        y1[k] = fs / (eb[k] - ea[k]);
+      }
+    }
     double track[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      while (seg[k] < last[k] && x1[k] <= t) {
-        const double* e = ev[k] + (++seg[k]);
-        x0[k] = x1[k];
-        y0[k] = y1[k];
-        x1[k] = (e[0] + e[1]) / 2.0 / fs;
-        y1[k] = fs / (e[1] - e[0]);
-      }
       const double s = (t - x0[k]) / (x1[k] - x0[k]);
       track[k] = y0[k] + s * (y1[k] - y0[k]);
     }
