@@ -298,7 +298,7 @@ struct Plan {
   size_t arena_bytes = 0;
   struct Layout {
     size_t meta, pcm, x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores,
-        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed;
+        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed, keys;
   } at{};
   int bank_ctas = 0;
   // Device pointers, set by Workspace::prepare: into the arena's copy of
@@ -649,6 +649,7 @@ struct Workspace {
     p->at.count = take(4 * B);
     p->at.jobs = take(sizeof(RefineJob) * size_t(p->capacity) * F);
     p->at.classes = take(sizeof(int) * (2 * kRefineClasses + 1));
+    p->at.keys = take(sizeof(ulonglong2) * size_t(p->per_group) * F);
     p->at.refined = take(8 * size_t(p->capacity) * F);
     p->at.scores = take(8 * size_t(p->capacity) * F);
     p->at.pruned = take(8 * size_t(p->capacity) * F);
@@ -750,6 +751,7 @@ struct Workspace {
     rb.class_cursor = rb.class_count + kRefineClasses;
     rb.total = rb.class_cursor + kRefineClasses;
     rb.jobs = ptr<RefineJob>(p.at.jobs);
+    rb.keys = ptr<ulonglong2>(p.at.keys);
     check(launch_refine(bv, rb, y, ptr<double>(p.at.cand), ptr<int>(p.at.count), F,
                         ptr<double>(p.at.refined), ptr<double>(p.at.scores), sms, p.refine_shape, s),
           "refine");
@@ -837,6 +839,7 @@ struct Workspace {
     rb.class_cursor = rb.class_count + kRefineClasses;
     rb.total = rb.class_cursor + kRefineClasses;
     rb.jobs = ptr<RefineJob>(p.at.jobs);
+    rb.keys = ptr<ulonglong2>(p.at.keys);
     const int64_t F = p.frame_off[p.clips];
     RefineShape best{};
     float best_ms = 0.0f;

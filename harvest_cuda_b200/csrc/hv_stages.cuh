@@ -127,6 +127,7 @@ struct RefineBuffers {
   int* class_cursor;   // [kRefineClasses]
   int* total;          // [1]
   RefineJob* jobs;     // [frames * capacity]
+  ulonglong2* keys;    // [frames * per_group] refinement key of every official candidate
 };
 // Launch shape of the refinement jobs: minimum resident 128-thread blocks per
 // SM the kernel instance is compiled for (1, 4 or 5; fewer registers per

@@ -21,11 +21,75 @@ __device__ __forceinline__ int size_class(int len) {
   return e < 2 ? 4 * e : 4 * e + ((len >> (e - 2)) & 3);
 }
 
+// GetRefinedF0 / GetMeanF0 / GetBaseIndex / GetMainWindow / GetDiffWindow /
+// GetSpectra / FixF0 (harvest.cpp:434-617) for one candidate. The reference
+// windows the waveform with a Blackman window and its centred difference,
+// takes two zero-padded FFTs of size n and reads at most six harmonic bins.
+// Only those bins are needed, so they are evaluated directly as DFT sums.
+// The window phasor advances by 2 pi / len per sample and each twiddle by
+// 2 pi k / n; both are re-anchored from exact values every kAnchor samples.
+constexpr int kAnchor = 64;
+
+// The discrete parameters of one candidate's refinement: window half length,
+// FFT size, first waveform index and the harmonic bins.
+struct CandidateWindow {
+  int half, len, n, base, harmonics;
+  int bin[6];
+  __device__ __forceinline__ CandidateWindow(double fs, double t, double f0c) {
+    half = static_cast<int>(1.5 * fs / f0c + 1.0);
+    len = 2 * half + 1;
+    n = 1 << (2 + (31 - __clz(len)));        // 2^(2 + floor(log2 len)), len odd
+    base = matlab_round((t + (-half) / fs) * fs + 0.001);
+    harmonics = imin(static_cast<int>(fs / 2.0 / f0c), 6);
+#pragma unroll
+    for (int h = 0; h < 6; ++h) bin[h] = h < harmonics ? matlab_round(f0c * n / fs * (h + 1)) : 0;
+  }
+};
+
+// Slot (row * per_group + j) of candidate j of frame f after overlap group
+// g (OverlapF0Candidates, harvest.cpp:417-429): from frame f (g = 0),
+// f - g (g = 1..3) or f + g - 3 (g = 4..6); -1 outside the clip.
+__device__ __forceinline__ int64_t sibling_slot(const BatchView& v, int64_t row0, int frames, int f, int g,
+                                                int j) {
+  const int src = g == 0 ? f : (g <= 3 ? f - g : f + (g - 3));
+  return src < 0 || src >= frames ? -1 : (row0 + src) * v.per_group + j;
+}
+
+// Refinement key of a candidate F0: its window half length, harmonic count
+// and bins, packed exactly. x = half << 32 | bin_0; y holds the harmonic
+// count and, per harmonic h >= 1, bin_h - (h + 1) bin_0 (within +-3, since
+// every bin rounds (h + 1) f0c n / fs) offset by 8 in 4 bits. Equal keys mean
+// equal windows and bins, hence bit-identical spectra at one frame. A delta
+// outside its field sets bit 63, and such keys are never taken as equal.
+__device__ __forceinline__ ulonglong2 refine_key(double fs, double f0c) {
+  const CandidateWindow cw(fs, 0.0, f0c);
+  unsigned long long y = static_cast<unsigned long long>(cw.harmonics);
+#pragma unroll
+  for (int h = 1; h < 6; ++h) {
+    const int delta = h < cw.harmonics ? cw.bin[h] - (h + 1) * cw.bin[0] : 0;
+    if (delta < -8 || delta > 7) y |= 1ull << 63;
+    y |= static_cast<unsigned long long>((delta + 8) & 15) << (4 * h);
+  }
+  return make_ulonglong2(static_cast<unsigned long long>(cw.half) << 32 | static_cast<unsigned int>(cw.bin[0]), y);
+}
+
+__device__ __forceinline__ bool same_key(ulonglong2 a, ulonglong2 b) {
+  return a.x == b.x && a.y == b.y && !(a.y >> 63);
+}
+
+__global__ void candidate_keys(BatchView v, const double* __restrict__ cand, int64_t slots,
+                               ulonglong2* __restrict__ keys) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= slots) return;
+  const double f0c = cand[i];
+  keys[i] = f0c > 0.0 ? refine_key(v.fs_r, f0c) : make_ulonglong2(0ull, 0ull);
+}
+
 template <bool kScatter>
 __global__ void __launch_bounds__(256)
 refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
-              int64_t total_frames, int* __restrict__ class_count, int* __restrict__ class_cursor,
-              RefineJob* __restrict__ jobs) {
+              const ulonglong2* __restrict__ keys, int64_t total_frames, int* __restrict__ class_count,
+              int* __restrict__ class_cursor, RefineJob* __restrict__ jobs) {
   __shared__ int s_count[kRefineClasses], s_base[kRefineClasses];
   for (int i = threadIdx.x; i < kRefineClasses; i += blockDim.x) s_count[i] = 0;
   __syncthreads();
@@ -37,11 +101,28 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
   if (cell < total_frames * v.capacity) {
     gf = cell / v.capacity;
     col = static_cast<int>(cell - gf * v.capacity);
-    f0c = overlapped_candidate(v, cand, count, gf, col);
-    if (f0c > 0.0) {
-      int half = static_cast<int>(1.5 * v.fs_r / f0c + 1.0);
-      cls = imin(size_class(2 * half + 1), kRefineClasses - 1);
-      rank = atomicAdd(&s_count[cls], 1);
+    const int c = owner(v.frame_off, v.clips, gf);
+    const int64_t row0 = v.frame_off[c];
+    const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
+    const int K = count[c];
+    if (col < 7 * K) {
+      const int g = col / K, j = col - g * K;
+      const int64_t slot = sibling_slot(v, row0, frames, f, g, j);
+      f0c = slot >= 0 ? cand[slot] : 0.0;
+      if (f0c > 0.0) {
+        // A sibling of lower group with the same key refines this cell.
+        const ulonglong2 key = keys[slot];
+        bool leader = true;
+        for (int g2 = 0; g2 < g && leader; ++g2) {
+          const int64_t o = sibling_slot(v, row0, frames, f, g2, j);
+          if (o >= 0 && cand[o] > 0.0 && same_key(key, keys[o])) leader = false;
+        }
+        if (leader) {
+          const int half = static_cast<int>(key.x >> 32);
+          cls = imin(size_class(2 * half + 1), kRefineClasses - 1);
+          rank = atomicAdd(&s_count[cls], 1);
+        }
+      }
     }
   }
   __syncthreads();
@@ -71,31 +152,6 @@ __global__ void refine_offsets(const int* __restrict__ class_count, int* __restr
   }
   *total = run;
 }
-
-// GetRefinedF0 / GetMeanF0 / GetBaseIndex / GetMainWindow / GetDiffWindow /
-// GetSpectra / FixF0 (harvest.cpp:434-617) for one candidate. The reference
-// windows the waveform with a Blackman window and its centred difference,
-// takes two zero-padded FFTs of size n and reads at most six harmonic bins.
-// Only those bins are needed, so they are evaluated directly as DFT sums.
-// The window phasor advances by 2 pi / len per sample and each twiddle by
-// 2 pi k / n; both are re-anchored from exact values every kAnchor samples.
-constexpr int kAnchor = 64;
-
-// The discrete parameters of one candidate's refinement: window half length,
-// FFT size, first waveform index and the harmonic bins.
-struct CandidateWindow {
-  int half, len, n, base, harmonics;
-  int bin[6];
-  __device__ __forceinline__ CandidateWindow(double fs, double t, double f0c) {
-    half = static_cast<int>(1.5 * fs / f0c + 1.0);
-    len = 2 * half + 1;
-    n = 1 << (2 + (31 - __clz(len)));        // 2^(2 + floor(log2 len)), len odd
-    base = matlab_round((t + (-half) / fs) * fs + 0.001);
-    harmonics = imin(static_cast<int>(fs / 2.0 / f0c), 6);
-#pragma unroll
-    for (int h = 0; h < 6; ++h) bin[h] = h < harmonics ? matlab_round(f0c * n / fs * (h + 1)) : 0;
-  }
-};
 
 // Visits the window's samples in order: body(i, w, dw, tr, ti) receives the
 // Blackman window w, the centred difference window dw and, per harmonic,
@@ -235,53 +291,81 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
   }
 }
 
-__device__ void refine_candidate(const double* __restrict__ y, int y_len, double fs, double t,
-                                 double f0c, double f0_floor, double f0_ceil, double& out_f0,
-                                 double& out_score) {
-  const CandidateWindow cw(fs, t, f0c);
-  HarmonicSpectra sp;
-  candidate_spectra(y, y_len, fs, t, cw, sp);
-  // FixF0 (harvest.cpp:507-536), same evaluation order.
-  double num = 0.0, den = 0.0, err = 0.0;
+// FixF0 (harvest.cpp:507-536) split in two, each sum in the reference's
+// order: the instantaneous frequencies and the refined F0 depend only on the
+// spectra; the score also depends on the candidate's initial F0. The
+// zeroing of RefineF0Candidates (harvest.cpp:610-614) follows the score.
+__device__ __forceinline__ double fix_f0_frequencies(const HarmonicSpectra& sp, const CandidateWindow& cw,
+                                                     double fs, double inst[6]) {
+  double num = 0.0, den = 0.0;
 #pragma unroll
   for (int h = 0; h < 6; ++h) {
-    if (h >= cw.harmonics) break;
+    inst[h] = 0.0;
+    if (h >= cw.harmonics) continue;
     const double power = sp.mr[h] * sp.mr[h] + sp.mi[h] * sp.mi[h];
     const double cross = sp.mr[h] * sp.di[h] - sp.mi[h] * sp.dr[h];
-    const double inst =
-        power == 0.0 ? 0.0 : static_cast<double>(cw.bin[h]) * fs / cw.n + cross / power * fs / 2.0 / kPi;
+    inst[h] = power == 0.0 ? 0.0 : static_cast<double>(cw.bin[h]) * fs / cw.n + cross / power * fs / 2.0 / kPi;
     const double amp = sqrt(power);
-    num += amp * inst;
+    num += amp * inst[h];
     den += amp * (h + 1.0);
-    err += fabs((inst / (h + 1.0) - f0c) / f0c);
   }
-  double refined = num / (den + kGuard);
-  double score = 1.0 / (err / cw.harmonics + kGuard);
-  if (refined < f0_floor || refined > f0_ceil || score < 2.5) refined = score = 0.0;  // :610-614
+  return num / (den + kGuard);
+}
+
+__device__ __forceinline__ void fix_f0_score(const double inst[6], int harmonics, double refined, double f0c,
+                                             double f0_floor, double f0_ceil, double& out_f0, double& out_score) {
+  double err = 0.0;
+#pragma unroll
+  for (int h = 0; h < 6; ++h)
+    if (h < harmonics) err += fabs((inst[h] / (h + 1.0) - f0c) / f0c);
+  double score = 1.0 / (err / harmonics + kGuard);
+  if (refined < f0_floor || refined > f0_ceil || score < 2.5) refined = score = 0.0;
   out_f0 = refined;
   out_score = score;
 }
 
 // One thread per job, grid-stride over the job list (longest windows first).
-// kMinBlocks caps registers so that that many 128-thread blocks fit on an
+// A job's spectra also serve every later overlap sibling (same candidate,
+// group g2 > g) with the same window and bins: those cells get FixF0 with
+// their own initial F0, which changes only the score. kMinBlocks caps registers so that that many 128-thread blocks fit on an
 // SM; the autotuner picks the instance and the grid (RefineShape).
 template <int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks)
 refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restrict__ jobs,
-            const int* __restrict__ total, double* __restrict__ refined, double* __restrict__ scores) {
-  const int count = *total;
-  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < count; idx += gridDim.x * blockDim.x) {
+            const int* __restrict__ total, const double* __restrict__ cand, const int* __restrict__ count,
+            const ulonglong2* __restrict__ keys, double* __restrict__ refined, double* __restrict__ scores) {
+  const int total_jobs = *total;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total_jobs; idx += gridDim.x * blockDim.x) {
     const RefineJob job = jobs[idx];
     const int64_t gf = job.key / kRefineColumns;
     const int col = static_cast<int>(job.key - gf * kRefineColumns);
     const int c = owner(v.frame_off, v.clips, gf);
-    const int f = static_cast<int>(gf - v.frame_off[c]);
+    const int64_t row0 = v.frame_off[c];
+    const int f = static_cast<int>(gf - row0);
     const int64_t y0 = v.y_off[c];
+    const double t = f * 1 / 1000.0;
+    const CandidateWindow cw(v.fs_r, t, job.f0c);
+    HarmonicSpectra sp;
+    candidate_spectra(y + y0, static_cast<int>(v.y_off[c + 1] - y0), v.fs_r, t, cw, sp);
+    double inst[6];
+    const double value = fix_f0_frequencies(sp, cw, v.fs_r, inst);
+    const int harmonics = cw.harmonics;
     double f0 = 0.0, score = 0.0;
-    refine_candidate(y + y0, static_cast<int>(v.y_off[c + 1] - y0), v.fs_r, f * 1 / 1000.0, job.f0c,
-                     v.f0_floor, v.f0_ceil, f0, score);
+    fix_f0_score(inst, harmonics, value, job.f0c, v.f0_floor, v.f0_ceil, f0, score);
     refined[gf * v.capacity + col] = f0;
     scores[gf * v.capacity + col] = score;
+    const int frames = static_cast<int>(v.frame_off[c + 1] - row0);
+    const int K = count[c], g = col / K, j = col - g * K;
+    const ulonglong2 key = keys[sibling_slot(v, row0, frames, f, g, j)];
+    for (int g2 = g + 1; g2 < 7; ++g2) {
+      const int64_t o = sibling_slot(v, row0, frames, f, g2, j);
+      if (o < 0) continue;
+      const double other = cand[o];
+      if (!(other > 0.0) || !same_key(key, keys[o])) continue;
+      fix_f0_score(inst, harmonics, value, other, v.f0_floor, v.f0_ceil, f0, score);
+      refined[gf * v.capacity + g2 * K + j] = f0;
+      scores[gf * v.capacity + g2 * K + j] = score;
+    }
   }
 }
 
@@ -363,17 +447,16 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
   if ((e = cudaMemsetAsync(refined, 0, sizeof(double) * cells, stream)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(scores, 0, sizeof(double) * cells, stream)) != cudaSuccess) return e;
   const unsigned grid = static_cast<unsigned>((cells + 255) / 256);
-  refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, total_frames, b.class_count,
+  const int64_t slots = total_frames * v.per_group;
+  candidate_keys<<<static_cast<unsigned>((slots + 255) / 256), 256, 0, stream>>>(v, cand, slots, b.keys);
+  refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.class_count,
                                                  b.class_cursor, b.jobs);
   refine_offsets<<<1, 32, 0, stream>>>(b.class_count, b.class_cursor, b.total);
-  refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, total_frames, b.class_count,
+  refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.class_count,
                                                 b.class_cursor, b.jobs);
   const unsigned job_grid = static_cast<unsigned>(sms * shape.blocks_per_sm);
-  switch (shape.min_blocks) {
-    case 4: refine_jobs<4><<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores); break;
-    case 5: refine_jobs<5><<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores); break;
-    default: refine_jobs<1><<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, refined, scores); break;
-  }
+  auto kernel = shape.min_blocks == 4 ? refine_jobs<4> : (shape.min_blocks == 5 ? refine_jobs<5> : refine_jobs<1>);
+  kernel<<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, cand, count, b.keys, refined, scores);
   return cudaGetLastError();
 }
 
