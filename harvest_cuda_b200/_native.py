@@ -54,6 +54,11 @@ SIGNATURES = {
     "hv_harvest_grad_backward": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
                                             ct.c_double, ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                             ct.c_void_p]),
+    "hv_band_count": (ct.c_int64, [ct.c_double, ct.c_double]),
+    "hv_raw_candidates": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double, ct.c_int,
+                                     ct.c_void_p, ct.c_void_p]),
+    "hv_raw_candidates_backward": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
+                                              ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
     "hv_clear_cache": (ct.c_int, []),
 }
 

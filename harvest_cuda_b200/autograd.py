@@ -29,7 +29,7 @@ import torch
 
 from . import _native
 
-__all__ = ["HarvestF0", "harvest_f0"]
+__all__ = ["HarvestF0", "harvest_f0", "RawCandidates", "raw_candidates"]
 
 
 def _settings(fs, f0_floor, f0_ceil, frame_period):
@@ -125,3 +125,73 @@ def harvest_f0(x, fs, f0_floor=71.0, f0_ceil=800.0, frame_period=5.0):
         return f0, times
     counts = _frames(offsets, int(fs), float(frame_period))
     return list(zip(torch.split(f0, counts), torch.split(times, counts)))
+
+
+class RawCandidates(torch.autograd.Function):
+    """``RawCandidates.apply(x, offsets, fs, f0_floor, f0_ceil)``: the band-pass
+    bank's per-band F0 candidates (WORLD's GetF0CandidateContour) of clips
+    packed in ``x`` as for ``HarvestF0``, as a ``(bands, frames)`` float64 CUDA
+    tensor (1 ms frames of all clips in order; 0 where a band has no
+    candidate). Differentiable with respect to ``x``: the fine positions of
+    the zero crossings and extrema move smoothly with the waveform, while the
+    events themselves, each frame's interpolation segments and the range
+    checks are held fixed. The backward pass runs the adjoint of the
+    band-pass bank, the interval detectors and the decimation on the GPU."""
+
+    @staticmethod
+    def forward(ctx, x, offsets, fs, f0_floor, f0_ceil):
+        fs, f0_floor, f0_ceil = int(fs), float(f0_floor), float(f0_ceil)
+        if x.dtype != torch.float64 or x.dim() != 1 or not x.is_cuda:
+            raise TypeError("x must be a 1-D float64 CUDA tensor")
+        offsets = tuple(int(o) for o in offsets)
+        if len(offsets) < 2 or offsets[0] != 0 or offsets[-1] != x.numel():
+            raise ValueError("offsets must start at 0 and end at x.numel()")
+        x = x.contiguous()
+        if not bool(torch.isfinite(x).all()):
+            raise ValueError("x must contain only finite samples")
+        device = x.device.index if x.device.index is not None else torch.cuda.current_device()
+        bands = int(_native.lib.hv_band_count(f0_floor, f0_ceil))
+        if bands < 1:
+            raise ValueError("invalid f0_floor/f0_ceil")
+        frames = sum(_frames(offsets, fs, 1.0))
+        raw = torch.empty((bands, frames), dtype=torch.float64, device=x.device)
+        offs = (ct.c_int64 * len(offsets))(*offsets)
+        _native.raise_for(_native.lib.hv_raw_candidates(
+            x.data_ptr(), offs, len(offsets) - 1, fs, f0_floor, f0_ceil, device, raw.data_ptr(),
+            _stream(x.device)))
+        ctx.save_for_backward(x)
+        ctx.args = (offsets, fs, f0_floor, f0_ceil, device)
+        return raw
+
+    @staticmethod
+    def backward(ctx, grad_raw):
+        (x,) = ctx.saved_tensors
+        offsets, fs, f0_floor, f0_ceil, device = ctx.args
+        grad_x = None
+        if ctx.needs_input_grad[0]:
+            grad_raw = grad_raw.to(torch.float64).contiguous()
+            grad_x = torch.empty_like(x)
+            offs = (ct.c_int64 * len(offsets))(*offsets)
+            _native.raise_for(_native.lib.hv_raw_candidates_backward(
+                x.data_ptr(), offs, len(offsets) - 1, fs, f0_floor, f0_ceil, device, grad_raw.data_ptr(),
+                grad_x.data_ptr(), _stream(x.device)))
+        return grad_x, None, None, None, None
+
+
+def raw_candidates(x, fs, f0_floor=71.0, f0_ceil=800.0):
+    """Differentiable per-band candidates of one clip (a ``(bands, frames)``
+    tensor) or of a list of clips (a list of such tensors, run as one batch)."""
+    single = torch.is_tensor(x)
+    clips = [x] if single else list(x)
+    if not clips:
+        raise ValueError("no clips")
+    offsets = [0]
+    for c in clips:
+        if not torch.is_tensor(c) or c.dim() != 1:
+            raise TypeError("each clip must be a 1-D float64 CUDA tensor")
+        offsets.append(offsets[-1] + c.numel())
+    packed = clips[0] if single else torch.cat(clips)
+    raw = RawCandidates.apply(packed, tuple(offsets), fs, f0_floor, f0_ceil)
+    if single:
+        return raw
+    return list(torch.split(raw, _frames(offsets, int(fs), 1.0), dim=1))

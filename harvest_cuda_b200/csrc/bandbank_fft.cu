@@ -159,6 +159,10 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
         }
       }
       __syncthreads();
+      if (v.dump) {
+        double* d = v.dump + (static_cast<int64_t>(b) * g.total_blocks + blk0 + j) * (g.valid + 2);
+        for (int q = tid; q < edge_end + 2; q += kFftThreads) d[q] = xs[q + div_run(q)];
+      }
       // Events: each thread scans a contiguous run of positions, counting in
       // the first pass; a block scan of the packed counts orders the runs;
       // the second pass writes the sub-sample edges of its hits.

@@ -243,12 +243,19 @@ struct BankTables {
   std::vector<double> taps_rev;
 };
 
+// Band-pass channels of HarvestGeneralBody (harvest.cpp:1161-1162): 40 per
+// octave between 0.9 f0_floor and 1.1 f0_ceil.
+int band_count(double floor, double ceil) {
+  const double lo = floor * 0.9, hi = ceil * 1.1;
+  return 1 + static_cast<int>(std::log(hi / lo) / kLog2 * 40.0);
+}
+
 BankTables make_bank(int fs, double floor, double ceil) {
   BankTables t;
   const int ratio = ratio_for(fs);
   const double fs_r = double(fs) / ratio;
-  const double lo = floor * 0.9, hi = ceil * 1.1;
-  t.bands = 1 + static_cast<int>(std::log(hi / lo) / kLog2 * 40.0);
+  const double lo = floor * 0.9;
+  t.bands = band_count(floor, ceil);
   const int mult = band_bank_tap_multiple();
   t.tap_off.push_back(0);
   for (int b = 0; b < t.bands; ++b) {
@@ -373,6 +380,8 @@ struct Workspace {
   uint64_t meta_owner = 0;   // plan whose tables are at the head of the arena
   void* metric_buf = nullptr;   // inputs and offsets of hv_compare_batch
   size_t metric_size = 0;
+  void* raw_buf = nullptr;      // band-bank dump and adjoint scratch of the per-band-candidate gradient
+  size_t raw_size = 0;
 
   explicit Workspace(int dev) : device(dev), ctx(dev) {
     ContextGuard g(ctx.get());
@@ -394,6 +403,7 @@ struct Workspace {
       device_banks.clear();
       if (arena) cudaFree(arena);
       if (metric_buf) cudaFree(metric_buf);
+      if (raw_buf) cudaFree(raw_buf);
       if (twiddles) cudaFree(twiddles);
       if (host_flag) cudaFreeHost(host_flag);
       for (auto& e : marks) if (e) cudaEventDestroy(e);
@@ -686,6 +696,23 @@ struct Workspace {
     return dv;
   }
 
+  static BankView bank_view(const Plan& p) {
+    BankView kv{};
+    kv.batch = batch_view(p);
+    kv.centre = p.d_centre; kv.half = p.d_half; kv.tap_off = p.d_tap_off; kv.taps_rev = p.d_taps;
+    kv.items = p.d_items; kv.item_count = static_cast<int>(p.items.size());
+    kv.max_pad_taps = p.bank->max_pad_taps; kv.total_frames = p.frame_off[p.clips];
+    kv.slot_capacity = p.slot_capacity;
+    return kv;
+  }
+
+  static FftBankGeometry fft_geometry(const Plan& p) {
+    const int run = 2 * ((p.fft_valid + 2 + 2 * 256 - 1) / (2 * 256));
+    // The event scan keeps one 32-bit hit mask per kind and thread run.
+    if (run > 32) throw RuntimeFailure("FFT band bank: event run longer than 32 positions");
+    return FftBankGeometry{p.bank->max_half, p.fft_valid, run, p.total_blocks, p.d_blk_off};
+  }
+
   ContourView contour_view(const Plan& p) const {
     ContourView cv{};
     cv.batch = batch_view(p);
@@ -722,19 +749,12 @@ struct Workspace {
     check(launch_check_finite(x, p.x_off[B], ptr<int>(p.at.flag), sms, s), "check_finite");
     enqueue_waveform(p, x, s);
     mark(1);
-    BankView kv{};
-    kv.batch = bv;
-    kv.centre = p.d_centre; kv.half = p.d_half; kv.tap_off = p.d_tap_off; kv.taps_rev = p.d_taps;
-    kv.items = p.d_items; kv.item_count = static_cast<int>(p.items.size());
-    kv.max_pad_taps = p.bank->max_pad_taps; kv.total_frames = F; kv.slot_capacity = p.slot_capacity;
+    const BankView kv = bank_view(p);
     check(cudaMemsetAsync(ptr<int>(p.at.queue), 0, 16, s), "memset");
     if (p.use_fft) {
-      const int run = 2 * ((p.fft_valid + 2 + 2 * 256 - 1) / (2 * 256));
-      // The event scan keeps one 32-bit hit mask per kind and thread run.
-      if (run > 32) throw RuntimeFailure("FFT band bank: event run longer than 32 positions");
-      FftBankGeometry geo{p.bank->max_half, p.fft_valid, run, p.total_blocks, p.d_blk_off};
-      check(launch_fft_bank(kv, geo, y, ptr<double>(p.at.bins), twiddles, p.filters, ptr<double2>(p.at.spectra),
-                            ptr<int>(p.at.queue), ptr<double>(p.at.slots), p.bank_ctas, ptr<double>(p.at.raw), s),
+      check(launch_fft_bank(kv, fft_geometry(p), y, ptr<double>(p.at.bins), twiddles, p.filters,
+                            ptr<double2>(p.at.spectra), ptr<int>(p.at.queue), ptr<double>(p.at.slots), p.bank_ctas,
+                            ptr<double>(p.at.raw), s),
             "band_bank_fft");
     } else {
       check(launch_band_bank(kv, y, ptr<double>(p.at.bins), ptr<int>(p.at.queue), ptr<double>(p.at.slots),
@@ -768,6 +788,72 @@ struct Workspace {
   // that run's candidates and contour scratch).
   void enqueue_tape(Plan& p, double* tape, cudaStream_t s) {
     check(launch_tape(contour_view(p), ptr<double>(p.at.cand), p.frame_off[p.clips], tape, s), "tape");
+  }
+
+  // Backward pass of the per-band-candidate gradient: dL/dx from
+  // dL/draw[band][frame]. Recomputes y, reruns the FFT band bank with its
+  // dump, then the band-bank adjoint, the transpose of the filters, and the
+  // DC-removal and decimation adjoints.
+  void enqueue_raw_backward(Plan& p, const double* x, const double* grad_raw, double* grad_x, cudaStream_t s) {
+    if (!p.use_fft)
+      throw InvalidArgument("the per-band candidate gradient needs the FFT band bank (f0_floor is too low)");
+    const int B = p.clips;
+    const int64_t F = p.frame_off[B], y_total = p.y_off[B];
+    const FftBankGeometry geo = fft_geometry(p);
+    const int ctas = p.bank_ctas;
+    const size_t dump_n = size_t(p.bands) * size_t(p.total_blocks) * size_t(p.fft_valid + 2);
+    const size_t gradf_n = size_t(p.bands) * size_t(y_total);
+    const size_t slot_n = size_t(ctas) * 4 * size_t(p.slot_capacity);
+    const size_t need = align_up(8 * dump_n) + align_up(8 * gradf_n) + 3 * align_up(8 * slot_n);
+    if (need > raw_size) {
+      check(cudaEventSynchronize(last), "cudaEventSynchronize");
+      check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
+      if (raw_buf) cudaFree(raw_buf);
+      raw_buf = nullptr;
+      raw_size = 0;
+      check(cudaMalloc(&raw_buf, need), "cudaMalloc(raw gradient)");
+      raw_size = need;
+    }
+    char* m = static_cast<char*>(raw_buf);
+    double* dump = reinterpret_cast<double*>(m);
+    double* grad_f = reinterpret_cast<double*>(m + align_up(8 * dump_n));
+    char* slots = m + align_up(8 * dump_n) + align_up(8 * gradf_n);
+    enqueue_waveform(p, x, s);
+    BankView kv = bank_view(p);
+    kv.dump = dump;
+    check(cudaMemsetAsync(ptr<int>(p.at.queue), 0, 16, s), "memset");
+    check(launch_fft_bank(kv, geo, ptr<double>(p.at.y), ptr<double>(p.at.bins), twiddles, p.filters,
+                          ptr<double2>(p.at.spectra), ptr<int>(p.at.queue), ptr<double>(p.at.slots), ctas,
+                          ptr<double>(p.at.raw), s),
+          "band_bank_fft");
+    check(cudaMemsetAsync(grad_f, 0, 8 * gradf_n, s), "memset");
+    check(cudaMemsetAsync(ptr<int>(p.at.queue), 0, 16, s), "memset");
+    RawAdjointView rv{};
+    rv.batch = batch_view(p);
+    rv.geo = geo;
+    rv.items = p.d_items; rv.item_count = static_cast<int>(p.items.size());
+    rv.centre = p.d_centre;
+    rv.dump = dump;
+    rv.grad_raw = grad_raw;
+    rv.total_frames = F;
+    rv.slot_capacity = p.slot_capacity;
+    rv.edges = reinterpret_cast<double*>(slots);
+    rv.where = reinterpret_cast<long long*>(slots + align_up(8 * slot_n));
+    rv.grad_edges = reinterpret_cast<double*>(slots + 2 * align_up(8 * slot_n));
+    rv.queue = ptr<int>(p.at.queue);
+    rv.grad_f = grad_f;
+    rv.y_total = y_total;
+    check(launch_raw_adjoint(rv, ctas, s), "raw_adjoint");
+    double* grad_y = ptr<double>(p.at.grad_y);
+    check(launch_band_correlate(rv.batch, grad_f, y_total, p.d_half, p.d_tap_off, p.d_taps, grad_y, s),
+          "band_correlate");
+    check(launch_remove_mean_adjoint(rv.batch, grad_y, s), "remove_mean_adjoint");
+    if (p.ratio > 1)
+      check(launch_decimate_adjoint(decimate_view(p), grad_y, ptr<double>(p.at.u), ptr<double>(p.at.states),
+                                    p.total_seg, grad_x, s),
+            "decimate_adjoint");
+    else
+      check(launch_copy(grad_y, p.x_off[B], grad_x, s), "copy");
   }
 
   // Backward pass of the F0 gradient: dL/dx for the clips at `x` from dL/df0
@@ -1291,6 +1377,48 @@ int hv_harvest_grad_backward(const double* x, const int64_t* offsets, int clips,
     ws.enqueue_backward(p, x + offsets[0], tape, grad_f0, grad_x + offsets[0], st);
     check(cudaEventRecord(ws.last, st), "cudaEventRecord");
   });
+}
+
+int hv_raw_candidates(const double* x, const int64_t* offsets, int clips, int fs, double f0_floor,
+                      double f0_ceil, int device, double* raw, void* stream) {
+  return guarded([&] {
+    validate_batch(offsets, clips, fs, f0_floor, f0_ceil, 5.0);
+    if (!x || !raw) throw InvalidArgument("null buffer");
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    Plan& p = ws.prepare(Settings{fs, f0_floor, f0_ceil, 5.0}, offsets, clips, st);
+    check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x + offsets[0], 8 * p.x_off[clips], cudaMemcpyDeviceToDevice, st),
+          "cudaMemcpy(x)");
+    ws.run(p, st, true, false);
+    check(cudaMemcpyAsync(raw, ws.ptr<double>(p.at.raw), 8 * size_t(p.bands) * size_t(p.frame_off[clips]),
+                          cudaMemcpyDeviceToDevice, st),
+          "cudaMemcpy(raw)");
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
+  });
+}
+
+int hv_raw_candidates_backward(const double* x, const int64_t* offsets, int clips, int fs, double f0_floor,
+                               double f0_ceil, int device, const double* grad_raw, double* grad_x, void* stream) {
+  return guarded([&] {
+    validate_batch(offsets, clips, fs, f0_floor, f0_ceil, 5.0);
+    if (!x || !grad_raw || !grad_x) throw InvalidArgument("null buffer");
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : cudaStreamLegacy;
+    Plan& p = ws.prepare(Settings{fs, f0_floor, f0_ceil, 5.0}, offsets, clips, st);
+    ws.enqueue_raw_backward(p, x + offsets[0], grad_raw, grad_x + offsets[0], st);
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
+  });
+}
+
+int64_t hv_band_count(double f0_floor, double f0_ceil) {
+  if (!(f0_floor > 0) || !(f0_ceil > f0_floor) || !std::isfinite(f0_ceil)) return -1;
+  return band_count(f0_floor, f0_ceil);
 }
 
 int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor, double f0_ceil, int device,

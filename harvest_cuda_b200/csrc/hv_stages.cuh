@@ -46,6 +46,11 @@ struct BankView {
   int max_pad_taps;          // max padded tap count over bands
   int64_t total_frames;
   int64_t slot_capacity;     // events per kind per CTA slot
+  // Optional (FFT bank only; null otherwise): every block's filtered samples
+  // as its event scan reads them, lookahead included, at
+  // dump[(band * total_blocks + block) * (valid + 2) + q], for the adjoint of
+  // the per-band candidates.
+  double* dump;
 };
 
 struct ContourView {
@@ -104,6 +109,29 @@ struct FftBankGeometry {
   int64_t total_blocks;
   const int64_t* blk_off;  // [clips + 1] block offsets
 };
+// Adjoint of the band bank for the per-band candidates (bank_adjoint.cu).
+struct RawAdjointView {
+  BatchView batch;
+  FftBankGeometry geo;
+  const int2* items;           // (clip, band), as the band bank's
+  int item_count;
+  const double* centre;        // [bands]
+  const double* dump;          // band bank dump (BankView::dump)
+  const double* grad_raw;      // [bands][total_frames] dL/draw
+  int64_t total_frames;
+  int64_t slot_capacity;       // events per kind per CTA
+  double* edges;               // per CTA [4][slot_capacity]: fine edges
+  long long* where;            // per CTA [4][slot_capacity]: block * (valid + 2) + q of each event
+  double* grad_edges;          // per CTA [4][slot_capacity]: dL/de
+  int* queue;
+  double* grad_f;              // [bands][y_total] dL/df_b, zeroed
+  int64_t y_total;
+};
+cudaError_t launch_raw_adjoint(const RawAdjointView& v, int ctas, cudaStream_t stream);
+cudaError_t launch_band_correlate(const BatchView& v, const double* grad_f, int64_t y_total, const int* half,
+                                  const int64_t* tap_off, const double* taps_rev, double* grad_y,
+                                  cudaStream_t stream);
+
 size_t fft_bank_smem_bytes();
 int fft_bank_block_length();
 int fft_bank_ctas_per_sm();

@@ -157,6 +157,28 @@ HV_API int hv_harvest_grad_backward(const double* x, const int64_t* offsets, int
                                     const double* tape, const double* grad_f0, double* grad_x,
                                     void* stream);
 
+/* Per-band candidates with a gradient (no reference counterpart). The
+ * band-pass bank's candidates (GetF0CandidateContour, reference
+ * third_party/world/src/harvest.cpp:240-293) of clips packed as for
+ * hv_harvest_batch, on device pointers: raw receives
+ * hv_band_count(f0_floor, f0_ceil) rows of sum_c hv_output_length(n_c, fs,
+ * 1.0) doubles (row b holds band b's candidate at every 1 ms frame of every
+ * clip, clips in order; 0 where the band has none).
+ * hv_raw_candidates_backward takes dL/draw in that layout and writes dL/dx
+ * (laid out like x): the fine zero-crossing and extremum positions, and so
+ * the candidates, are smooth in x while the events themselves, each frame's
+ * interpolation segments and the range checks are held fixed. It
+ * recomputes the waveform and reruns the band bank, and needs the FFT band
+ * bank (HV_INVALID_ARGUMENT for floors so low that the direct FIR is used).
+ * WORLD's final-bin term is held fixed in the derivative. Streams as
+ * hv_harvest_grad_forward. */
+HV_API int64_t hv_band_count(double f0_floor, double f0_ceil);
+HV_API int hv_raw_candidates(const double* x, const int64_t* offsets, int clips, int fs, double f0_floor,
+                             double f0_ceil, int device, double* raw, void* stream);
+HV_API int hv_raw_candidates_backward(const double* x, const int64_t* offsets, int clips, int fs,
+                                      double f0_floor, double f0_ceil, int device, const double* grad_raw,
+                                      double* grad_x, void* stream);
+
 /* Diagnostic: runs hv_harvest on one clip and copies the intermediate stage
  * buffers to host memory, for stage-by-stage parity tests. Any pointer may
  * be NULL. Shapes (row-major, frames = analysis frames on the 1 ms grid,

@@ -140,3 +140,57 @@ def test_gradient_matches_finite_differences(gpu):
     assert skipped <= 4
     assert worst[1e-6] <= 1e-5, worst
     assert worst[1e-5] <= 1e-6, worst
+
+
+def test_raw_candidates_forward_is_the_pipelines(gpu):
+    torch = _torch()
+    x = signals.glide_clip(1.2, 16000, seed=4)[0]
+    raw = autograd.raw_candidates(torch.from_numpy(x).cuda(), 16000).cpu().numpy()
+    want = hv.api.stages(x, 16000)["raw"]
+    assert raw.shape == want.shape
+    assert np.array_equal(raw, want)
+
+
+def test_raw_candidate_gradient_matches_finite_differences(gpu):
+    """The band-bank adjoint (per-band candidates) against central
+    differences of the forward pass, at eps 1e-6 and 1e-5, errors measured
+    against the gradient's scale as for the F0 gradient."""
+    torch = _torch()
+    fs, per_clip = 16000, 12
+    x = signals.glide_clip(1.5, fs, seed=31)[0]
+    xt = torch.from_numpy(x.copy()).cuda().requires_grad_(True)
+    raw = autograd.raw_candidates(xt, fs)
+    mask = (raw.detach() != 0)
+    rng = np.random.default_rng(8)
+    weights = torch.from_numpy(rng.normal(size=tuple(raw.shape))).cuda() * mask
+    (raw * weights).sum().backward()
+    grad = xt.grad.cpu().numpy()
+    scale = np.abs(grad).max()
+    assert scale > 0
+    w = weights.cpu().numpy()
+    base = raw.detach().cpu().numpy()
+    positions = rng.choice(np.arange(int(0.3 * fs), int(1.2 * fs)), per_clip, replace=False)
+    worst = {1e-6: 0.0, 1e-5: 0.0}
+    skipped = 0
+    for eps in (1e-6, 1e-5):
+        batch = []
+        for p in positions:
+            for step in (eps, -eps):
+                xp = x.copy()
+                xp[p] += step
+                batch.append(torch.from_numpy(xp).cuda())
+        outs = [r.cpu().numpy() for r in autograd.raw_candidates(batch, fs)]
+        for k, p in enumerate(positions):
+            up, down = outs[2 * k], outs[2 * k + 1]
+            if not (np.array_equal(up != 0, base != 0) and np.array_equal(down != 0, base != 0)):
+                skipped += 1
+                continue
+            central = np.sum((up - down) * w) / (2 * eps)
+            curvature = np.sum((up - 2 * base + down) * w) / eps
+            if abs(curvature) > 1e-3 * max(abs(central), scale * 1e-3):
+                skipped += 1
+                continue
+            worst[eps] = max(worst[eps], abs(grad[p] - central) / scale)
+    assert skipped <= 6, skipped
+    assert worst[1e-6] <= 1e-5, worst
+    assert worst[1e-5] <= 1e-6, worst
