@@ -23,7 +23,8 @@ namespace hv {
 
 constexpr int kHalfN = kFftN;  // M: complex points per real block
 
-// tw[t] = e^{-2 pi i t / 8192}.
+// tw[t] = e^{-2 pi i t / 8192}. The refinement reads the same table.
+static_assert(kRealN == kTwiddleN, "the twiddle table has one entry per real block sample");
 __global__ void make_twiddles(double2* __restrict__ tw) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= kRealN) return;

@@ -772,6 +772,7 @@ struct Workspace {
     rb.total = rb.class_cursor + kRefineClasses;
     rb.jobs = ptr<RefineJob>(p.at.jobs);
     rb.keys = ptr<ulonglong2>(p.at.keys);
+    rb.twiddles = twiddles;
     check(launch_refine(bv, rb, y, ptr<double>(p.at.cand), ptr<int>(p.at.count), F,
                         ptr<double>(p.at.refined), ptr<double>(p.at.scores), sms, p.refine_shape, s),
           "refine");
@@ -875,7 +876,7 @@ struct Workspace {
     check(launch_contour_adjoint(gv, s), "contour_adjoint");
     double* grad_y = ptr<double>(p.at.grad_y);
     check(cudaMemsetAsync(grad_y, 0, 8 * p.y_off[B], s), "memset");
-    check(launch_refine_adjoint(bv, ptr<double>(p.at.y), tape, gv.grad_fixed, F, grad_y, sms, s),
+    check(launch_refine_adjoint(bv, ptr<double>(p.at.y), tape, gv.grad_fixed, F, twiddles, grad_y, sms, s),
           "refine_adjoint");
     check(launch_remove_mean_adjoint(bv, grad_y, s), "remove_mean_adjoint");
     if (p.ratio > 1)
@@ -926,6 +927,7 @@ struct Workspace {
     rb.total = rb.class_cursor + kRefineClasses;
     rb.jobs = ptr<RefineJob>(p.at.jobs);
     rb.keys = ptr<ulonglong2>(p.at.keys);
+    rb.twiddles = twiddles;
     const int64_t F = p.frame_off[p.clips];
     RefineShape best{};
     float best_ms = 0.0f;

@@ -132,6 +132,9 @@ cudaError_t launch_band_correlate(const BatchView& v, const double* grad_f, int6
                                   const int64_t* tap_off, const double* taps_rev, double* grad_y,
                                   cudaStream_t stream);
 
+// Entries of the workspace twiddle table e^{-2 pi i t / kTwiddleN} (the FFT
+// band bank's real block length).
+constexpr int kTwiddleN = 8192;
 size_t fft_bank_smem_bytes();
 int fft_bank_block_length();
 int fft_bank_ctas_per_sm();
@@ -156,6 +159,7 @@ struct RefineBuffers {
   int* total;          // [1]
   RefineJob* jobs;     // [frames * capacity]
   ulonglong2* keys;    // [frames * per_group] refinement key of every official candidate
+  const double2* twiddles;  // [kTwiddleN] e^{-2 pi i t / kTwiddleN}
 };
 // Launch shape of the refinement jobs: minimum resident 128-thread blocks per
 // SM the kernel instance is compiled for (1, 4 or 5; fewer registers per
@@ -178,8 +182,8 @@ cudaError_t launch_tape(const ContourView& v, const double* cand, int64_t total_
                         cudaStream_t stream);
 cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream);
 cudaError_t launch_refine_adjoint(const BatchView& v, const double* y, const double* tape,
-                                  const double* grad_fixed, int64_t total_frames, double* grad_y, int sms,
-                                  cudaStream_t stream);
+                                  const double* grad_fixed, int64_t total_frames, const double2* tw,
+                                  double* grad_y, int sms, cudaStream_t stream);
 cudaError_t launch_remove_mean_adjoint(const BatchView& v, double* grad_y, cudaStream_t stream);
 cudaError_t launch_decimate_adjoint(const DecimateView& v, const double* grad_y, double* u, double* states,
                                     int64_t segments, double* grad_x, cudaStream_t stream);

@@ -4,13 +4,14 @@
 // every frame with a Blackman window of about 3 fs / f0 samples, so the work
 // per candidate varies by two orders of magnitude. The stage therefore runs
 // as three steps:
-//   1. bucket: every (frame, column) slot applies OverlapF0Candidates
-//      (harvest.cpp:417-429) on the fly and counts its nonzero candidate in
-//      a quarter-octave class of its window length;
+//   1. bucket: one thread per (frame, official candidate) applies
+//      OverlapF0Candidates (harvest.cpp:417-429) on the fly to that
+//      candidate's seven overlap cells and counts each cell that needs its
+//      own spectra in a quarter-octave class of its window length;
 //   2. scatter: the same walk writes (f0, frame, column) jobs into one list
 //      ordered by class, longest windows first;
 //   3. refine: one thread per job, so the 32 lanes of a warp run windows of
-//      nearly the same length; outputs go to the job's own slot.
+//      nearly the same length; outputs go to the job's own cell.
 #include "hv_stages.cuh"
 
 namespace hv {
@@ -85,6 +86,12 @@ __global__ void candidate_keys(BatchView v, const double* __restrict__ cand, int
   keys[i] = f0c > 0.0 ? refine_key(v.fs_r, f0c) : make_ulonglong2(0ull, 0ull);
 }
 
+// One thread per (frame, official candidate j): the seven overlap cells of
+// column j (groups g = 0..6) at this frame. A cell is a job when its
+// candidate is nonzero and no lower group of the same j holds a candidate
+// with the same key; the leader's job also serves those later siblings.
+// Pass 1 (kScatter = false) counts jobs per window-length class, pass 2
+// writes them at the class offsets.
 template <bool kScatter>
 __global__ void __launch_bounds__(256)
 refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
@@ -93,34 +100,35 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
   __shared__ int s_count[kRefineClasses], s_base[kRefineClasses];
   for (int i = threadIdx.x; i < kRefineClasses; i += blockDim.x) s_count[i] = 0;
   __syncthreads();
-  int64_t cell = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  int cls = -1, rank = 0;
-  double f0c = 0.0;
+  const int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  int cls[7], rank[7];
+  double f0[7];
   int64_t gf = 0;
-  int col = 0;
-  if (cell < total_frames * v.capacity) {
-    gf = cell / v.capacity;
-    col = static_cast<int>(cell - gf * v.capacity);
+  int K = 0, j = 0;
+#pragma unroll
+  for (int g = 0; g < 7; ++g) cls[g] = -1;
+  if (item < total_frames * v.per_group) {
+    gf = item / v.per_group;
+    j = static_cast<int>(item - gf * v.per_group);
     const int c = owner(v.frame_off, v.clips, gf);
-    const int64_t row0 = v.frame_off[c];
-    const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
-    const int K = count[c];
-    if (col < 7 * K) {
-      const int g = col / K, j = col - g * K;
-      const int64_t slot = sibling_slot(v, row0, frames, f, g, j);
-      f0c = slot >= 0 ? cand[slot] : 0.0;
-      if (f0c > 0.0) {
-        // A sibling of lower group with the same key refines this cell.
-        const ulonglong2 key = keys[slot];
-        bool leader = true;
-        for (int g2 = 0; g2 < g && leader; ++g2) {
-          const int64_t o = sibling_slot(v, row0, frames, f, g2, j);
-          if (o >= 0 && cand[o] > 0.0 && same_key(key, keys[o])) leader = false;
-        }
+    K = count[c];
+    if (j < K) {
+      const int64_t row0 = v.frame_off[c];
+      const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
+      ulonglong2 key[7];
+#pragma unroll
+      for (int g = 0; g < 7; ++g) {
+        const int64_t slot = sibling_slot(v, row0, frames, f, g, j);
+        f0[g] = slot >= 0 ? cand[slot] : 0.0;
+        key[g] = f0[g] > 0.0 ? keys[slot] : make_ulonglong2(0ull, 0ull);
+        bool leader = f0[g] > 0.0;
+#pragma unroll
+        for (int g2 = 0; g2 < g; ++g2)
+          if (f0[g2] > 0.0 && same_key(key[g], key[g2])) leader = false;
         if (leader) {
-          const int half = static_cast<int>(key.x >> 32);
-          cls = imin(size_class(2 * half + 1), kRefineClasses - 1);
-          rank = atomicAdd(&s_count[cls], 1);
+          const int half = static_cast<int>(key[g].x >> 32);
+          cls[g] = imin(size_class(2 * half + 1), kRefineClasses - 1);
+          rank[g] = atomicAdd(&s_count[cls[g]], 1);
         }
       }
     }
@@ -133,11 +141,13 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
   }
   if (!kScatter) return;
   __syncthreads();
-  if (cls >= 0) {
+#pragma unroll
+  for (int g = 0; g < 7; ++g) {
+    if (cls[g] < 0) continue;
     RefineJob job;
-    job.f0c = f0c;
-    job.key = gf * kRefineColumns + col;
-    jobs[s_base[cls] + rank] = job;
+    job.f0c = f0[g];
+    job.key = gf * kRefineColumns + g * K + j;
+    jobs[s_base[cls[g]] + rank[g]] = job;
   }
 }
 
@@ -208,33 +218,35 @@ struct HarmonicSpectra {
   double mr[6], mi[6], dr[6], di[6];
 };
 
-// The bin sums are Goertzel recurrences in Reinsch's form, which keeps the
-// error near that of a direct sum for angles near 0 (and, in its mirrored
-// form, near pi): with theta = 2 pi bin / n,
-//   cos theta >= 0:  q += lambda s + x,  s += q,   lambda = -4 sin^2(theta / 2)
-//   cos theta <  0:  q  = lambda s - q + x,  s = q - s,  lambda = 4 cos^2(theta / 2)
-// written as q = lambda s + sigma q + x, s = sigma s + q with sigma = +-1.
-// After the window, s_{N-1} = s and s_{N-2} = sigma (s - q), and
-// X = e^{-i theta (N-1)} (s_{N-1} - e^{-i theta} s_{N-2}). Per harmonic and
-// sample this is 3 operations per windowed sequence, against 4 accumulations
-// and a 4-operation twiddle rotation for the direct sum.
+// e^{-2 pi i m / n} for 0 <= m < n, n a power of two: from the workspace
+// table tw[t] = e^{-2 pi i t / kTwiddleN} when n <= kTwiddleN (the argument
+// 2 m / n is then exactly 2 t / kTwiddleN, so the entry is the value sincospi
+// would give), else computed.
+__device__ __forceinline__ double2 bin_twiddle(const double2* __restrict__ tw, long long m, int n) {
+  if (n <= kTwiddleN) return __ldg(&tw[m * (kTwiddleN / n)]);
+  double s, c;
+  sincospi(2.0 * static_cast<double>(m) / n, &s, &c);
+  return make_double2(c, -s);
+}
+
+// The bin sums are Goertzel recurrences, one for the windowed and one for
+// the difference-windowed waveform per harmonic: with theta = 2 pi bin / n,
+//   s_i = x_i + 2 cos(theta) s_{i-1} - s_{i-2},
+//   X = e^{-i theta (N-1)} (s_{N-1} - e^{-i theta} s_{N-2}).
+// Per harmonic and sample that is 2 operations per sequence, one multiply-add
+// on the dependency chain. The rounding error grows as theta nears 0; at the
+// longest windows of a 50 Hz floor at 8 kHz (483 samples, n = 1024) it stays
+// below 2.5e-13 of sum |x| (against an extended-precision sum), far inside
+// the F0 tolerance, and the refined F0 moves by less than that.
 __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, int y_len, double fs,
-                                                  double t, const CandidateWindow& cw, HarmonicSpectra& sp) {
+                                                  double t, const CandidateWindow& cw,
+                                                  const double2* __restrict__ tw, HarmonicSpectra& sp) {
   const int len = cw.len, n = cw.n;
-  double lam[6], sig[6], qa[6], sa[6], qd[6], sd[6];
+  double c2[6], a1[6], a2[6], d1[6], d2[6];
 #pragma unroll
   for (int h = 0; h < 6; ++h) {
-    const double frac = static_cast<double>(cw.bin[h]) / n;      // theta / (2 pi)
-    if (4 * cw.bin[h] <= n) {
-      const double half = sinpi(frac);
-      lam[h] = -4.0 * half * half;
-      sig[h] = 1.0;
-    } else {
-      const double half = cospi(frac);
-      lam[h] = 4.0 * half * half;
-      sig[h] = -1.0;
-    }
-    qa[h] = sa[h] = qd[h] = sd[h] = 0.0;
+    c2[h] = 2.0 * bin_twiddle(tw, cw.bin[h], n).x;
+    a1[h] = a2[h] = d1[h] = d2[h] = 0.0;
   }
   const double span = (2.0 * cw.half + 1.0) / fs;
   double ds, dc;
@@ -249,21 +261,27 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
   double w_cur = 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0);
   const bool inside = cw.base - 1 >= 0 && cw.base - 1 + len <= y_len;
   const double* yb = y + (cw.base - 1);
-  for (int i0 = 0; i0 < len; i0 += kAnchor) {
-    phase(i0 + 1, nc, ns);
-    const int i1 = imin(i0 + kAnchor, len);
-    for (int i = i0; i < i1; ++i) {
-      const double w_next = (i + 1 < len) ? 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0) : 0.0;
-      const double dw = -(w_next - w_prev) / 2.0;
-      const double xs = inside ? yb[i] : y[imax(0, imin(y_len - 1, cw.base + i - 1))];
-      const double a = xs * w_cur, d = xs * dw;
+  auto accumulate = [&](int i, double w, double dw) {
+    const double xs = inside ? yb[i] : y[imax(0, imin(y_len - 1, cw.base + i - 1))];
+    const double a = xs * w, d = xs * dw;
 #pragma unroll
-      for (int h = 0; h < 6; ++h) {
-        qa[h] = fma(lam[h], sa[h], fma(sig[h], qa[h], a));
-        sa[h] = fma(sig[h], sa[h], qa[h]);
-        qd[h] = fma(lam[h], sd[h], fma(sig[h], qd[h], d));
-        sd[h] = fma(sig[h], sd[h], qd[h]);
-      }
+    for (int h = 0; h < 6; ++h) {
+      const double na = fma(c2[h], a1[h], a - a2[h]);
+      a2[h] = a1[h];
+      a1[h] = na;
+      const double nd = fma(c2[h], d1[h], d - d2[h]);
+      d2[h] = d1[h];
+      d1[h] = nd;
+    }
+  };
+  // Samples 0 .. len - 2; the last one, whose next window value is 0, after.
+  for (int i0 = 0; i0 < len - 1; i0 += kAnchor) {
+    phase(i0 + 1, nc, ns);
+    const int i1 = imin(i0 + kAnchor, len - 1);
+#pragma unroll 2
+    for (int i = i0; i < i1; ++i) {
+      const double w_next = 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0);
+      accumulate(i, w_cur, -(w_next - w_prev) / 2.0);
       const double rc = fma(nc, dc, -ns * ds);
       ns = fma(nc, ds, ns * dc);
       nc = rc;
@@ -271,20 +289,20 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
       w_cur = w_next;
     }
   }
+  accumulate(len - 1, w_cur, -(0.0 - w_prev) / 2.0);
 #pragma unroll
   for (int h = 0; h < 6; ++h) {
-    double st, ct, sp_, cp;
-    sincospi(2.0 * cw.bin[h] / n, &st, &ct);
-    const long long m = (static_cast<long long>(cw.bin[h]) * (len - 1)) % n;
-    sincospi(-2.0 * static_cast<double>(m) / n, &sp_, &cp);
+    const double2 step = bin_twiddle(tw, cw.bin[h], n);                        // e^{-i theta}
+    const double2 rot = bin_twiddle(tw, (static_cast<long long>(cw.bin[h]) * (len - 1)) & (n - 1), n);
+    const double ct = step.x, st = -step.y, cp = rot.x, sp_ = rot.y;
     // a sequence
-    double s2 = sig[h] * (sa[h] - qa[h]);
-    double re = sa[h] - ct * s2, im = st * s2;
+    double s2 = a2[h];
+    double re = a1[h] - ct * s2, im = st * s2;
     sp.mr[h] = re * cp - im * sp_;
     sp.mi[h] = re * sp_ + im * cp;
     // d sequence
-    s2 = sig[h] * (sd[h] - qd[h]);
-    re = sd[h] - ct * s2;
+    s2 = d2[h];
+    re = d1[h] - ct * s2;
     im = st * s2;
     sp.dr[h] = re * cp - im * sp_;
     sp.di[h] = re * sp_ + im * cp;
@@ -333,7 +351,8 @@ template <int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks)
 refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restrict__ jobs,
             const int* __restrict__ total, const double* __restrict__ cand, const int* __restrict__ count,
-            const ulonglong2* __restrict__ keys, double* __restrict__ refined, double* __restrict__ scores) {
+            const ulonglong2* __restrict__ keys, const double2* __restrict__ tw, double* __restrict__ refined,
+            double* __restrict__ scores) {
   const int total_jobs = *total;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total_jobs; idx += gridDim.x * blockDim.x) {
     const RefineJob job = jobs[idx];
@@ -346,7 +365,7 @@ refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restri
     const double t = f * 1 / 1000.0;
     const CandidateWindow cw(v.fs_r, t, job.f0c);
     HarmonicSpectra sp;
-    candidate_spectra(y + y0, static_cast<int>(v.y_off[c + 1] - y0), v.fs_r, t, cw, sp);
+    candidate_spectra(y + y0, static_cast<int>(v.y_off[c + 1] - y0), v.fs_r, t, cw, tw, sp);
     double inst[6];
     const double value = fix_f0_frequencies(sp, cw, v.fs_r, inst);
     const int harmonics = cw.harmonics;
@@ -379,7 +398,8 @@ refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restri
 // pass); the frame's share of dL/dy is added with atomics.
 __global__ void __launch_bounds__(128)
 refine_adjoint(BatchView v, const double* __restrict__ y, const double* __restrict__ tape,
-               const double* __restrict__ grad_fixed, int64_t total_frames, double* __restrict__ grad_y) {
+               const double* __restrict__ grad_fixed, int64_t total_frames, const double2* __restrict__ tw,
+               double* __restrict__ grad_y) {
   for (int64_t gf = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gf < total_frames;
        gf += (int64_t)gridDim.x * blockDim.x) {
     const double g = grad_fixed[gf];
@@ -394,7 +414,7 @@ refine_adjoint(BatchView v, const double* __restrict__ y, const double* __restri
     const double fs = v.fs_r, t = f * 1 / 1000.0;
     const CandidateWindow cw(fs, t, f0c);
     HarmonicSpectra sp;
-    candidate_spectra(y + y0, y_len, fs, t, cw, sp);
+    candidate_spectra(y + y0, y_len, fs, t, cw, tw, sp);
     double num = 0.0, den = 0.0, amp[6], inst[6];
 #pragma unroll
     for (int h = 0; h < 6; ++h) {
@@ -446,9 +466,9 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
   if ((e = cudaMemsetAsync(b.class_count, 0, sizeof(int) * kRefineClasses, stream)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(refined, 0, sizeof(double) * cells, stream)) != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(scores, 0, sizeof(double) * cells, stream)) != cudaSuccess) return e;
-  const unsigned grid = static_cast<unsigned>((cells + 255) / 256);
   const int64_t slots = total_frames * v.per_group;
-  candidate_keys<<<static_cast<unsigned>((slots + 255) / 256), 256, 0, stream>>>(v, cand, slots, b.keys);
+  const unsigned grid = static_cast<unsigned>((slots + 255) / 256);
+  candidate_keys<<<grid, 256, 0, stream>>>(v, cand, slots, b.keys);
   refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.class_count,
                                                  b.class_cursor, b.jobs);
   refine_offsets<<<1, 32, 0, stream>>>(b.class_count, b.class_cursor, b.total);
@@ -456,16 +476,16 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
                                                 b.class_cursor, b.jobs);
   const unsigned job_grid = static_cast<unsigned>(sms * shape.blocks_per_sm);
   auto kernel = shape.min_blocks == 4 ? refine_jobs<4> : (shape.min_blocks == 5 ? refine_jobs<5> : refine_jobs<1>);
-  kernel<<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, cand, count, b.keys, refined, scores);
+  kernel<<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, cand, count, b.keys, b.twiddles, refined, scores);
   return cudaGetLastError();
 }
 
 cudaError_t launch_refine_adjoint(const BatchView& v, const double* y, const double* tape,
-                                  const double* grad_fixed, int64_t total_frames, double* grad_y, int sms,
-                                  cudaStream_t stream) {
+                                  const double* grad_fixed, int64_t total_frames, const double2* tw,
+                                  double* grad_y, int sms, cudaStream_t stream) {
   const int64_t blocks = (total_frames + 127) / 128;
   refine_adjoint<<<static_cast<unsigned>(blocks < sms * 8 ? blocks : sms * 8), 128, 0, stream>>>(
-      v, y, tape, grad_fixed, total_frames, grad_y);
+      v, y, tape, grad_fixed, total_frames, tw, grad_y);
   return cudaGetLastError();
 }
 
