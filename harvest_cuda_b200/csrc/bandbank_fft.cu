@@ -118,9 +118,13 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
                     static_cast<double>(kRealN) / n, red, c0, c1r, c1i);
     const double2* G = filters + static_cast<int64_t>(b) * (kHalfN + 1);
     const int64_t blk0 = g.blk_off[c], blocks = g.blk_off[c + 1] - blk0;
-    // e^{-2 pi i 256 / n}: the step of this thread's correction phasor.
-    double step_s, step_c;
-    sincospi(2.0 * kFftThreads / n, &step_s, &step_c);
+    FinalBinTerm fb;
+    fb.c0 = c0;
+    fb.c1r = c1r;
+    fb.c1i = c1i;
+    fb.n = n;
+    sincospi(2.0 / n, &fb.step1_s, &fb.step1_c);
+    sincospi(2.0 * 512 / n, &fb.step512_s, &fb.step512_c);
     int count[4] = {0, 0, 0, 0};
     for (int64_t j = 0; j < blocks; ++j) {
       const double2* Y = spectra + (blk0 + j) * (kHalfN + 1);
@@ -140,26 +144,14 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
       __syncthreads();
       stockham_pass<+1>(buf, tw, 1);
       stockham_pass<+1>(buf, tw, 16);
-      inverse_last_pass_to_runs(buf, tw, 2 * H, div_run);
-      // Output i = j V + q (block sample 2H + q) now sits at lin[q + q / run].
-      // Add WORLD's final-bin term at its unnormalised index i + half + 1.
+      // Output i = j V + q (block sample 2H + q) lands at lin[q + q / run],
+      // plus WORLD's final-bin term at its unnormalised index i + half + 1.
       const int64_t o = j * g.valid;
       const int edge_end = static_cast<int>(min(static_cast<int64_t>(g.valid), y_len - 1 - o));
       const int peak_end = static_cast<int>(min(static_cast<int64_t>(g.valid), y_len - 2 - o));
-      {
-        const int64_t q0 = o + half + 1 + tid;
-        double ps, pc;
-        sincospi(2.0 * static_cast<double>(q0 % n) / n, &ps, &pc);
-        for (int q = tid; q < edge_end + 2; q += kFftThreads) {
-          const int64_t qq = o + half + 1 + q;
-          const double corr = c0 + 2.0 * (c1r * pc + c1i * ps);
-          xs[q + div_run(q)] += (qq & 1) ? -corr : corr;
-          const double nc = fma(pc, step_c, -ps * step_s);
-          ps = fma(pc, step_s, ps * step_c);
-          pc = nc;
-        }
-      }
-      __syncthreads();
+      fb.origin = o + half + 1;
+      fb.limit = edge_end + 2;
+      inverse_last_pass_to_runs(buf, tw, 2 * H, div_run, fb);
       if (v.dump) {
         double* d = v.dump + (static_cast<int64_t>(b) * g.total_blocks + blk0 + j) * (g.valid + 2);
         for (int q = tid; q < edge_end + 2; q += kFftThreads) d[q] = xs[q + div_run(q)];

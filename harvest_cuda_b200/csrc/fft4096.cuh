@@ -119,12 +119,25 @@ struct RunDivider {
   }
 };
 
+// WORLD's final-bin term for the samples of one block: sample q (absolute
+// index origin + q of the unnormalised output) gets
+// (-1)^(origin + q) (c0 + 2 (c1r cos phi + c1i sin phi)), phi = 2 pi (origin + q) / n,
+// for q < limit; n is a power of two.
+struct FinalBinTerm {
+  double c0, c1r, c1i;
+  long long origin;
+  int n, limit;
+  double step1_c, step1_s;      // e^{2 pi i / n}
+  double step512_c, step512_s;  // e^{2 pi i 512 / n}
+};
+
 // Last pass of an inverse transform whose result is read as 8192 real
 // samples x[2m] = Re z[m], x[2m+1] = Im z[m]: instead of storing z in natural
 // order it stores samples p >= first into lin[(p - first) + (p - first) / run],
-// one pad slot per `run` samples, the layout the event scan reads.
+// one pad slot per `run` samples, the layout the event scan reads, with the
+// final-bin term added on the way.
 __device__ __forceinline__ void inverse_last_pass_to_runs(double2* buf, const double2* __restrict__ tw,
-                                                          int first, RunDivider run) {
+                                                          int first, RunDivider run, const FinalBinTerm& fb) {
   const int j = threadIdx.x;
   const int ls = 256;
   const int k = j & (ls - 1);
@@ -139,14 +152,39 @@ __device__ __forceinline__ void inverse_last_pass_to_runs(double2* buf, const do
     wm = cmul(wm, w);
   }
   dft16<+1>(x);
+  const int out0 = (j - k) * 16 + k;
+  // Phasor of this thread's first (even) sample; its samples advance by 512.
+  double pc, ps;
+  {
+    const long long r = (fb.origin + 2 * out0 - first) & (fb.n - 1);
+    sincospi(2.0 * static_cast<double>(r) / fb.n, &ps, &pc);
+  }
+  const bool odd = (fb.origin - first) & 1;   // parity of origin + p for even p (first is even)
   __syncthreads();
   double* lin = reinterpret_cast<double*>(buf);
-  const int out0 = (j - k) * 16 + k;
 #pragma unroll
   for (int m = 0; m < 16; ++m) {
     const int p = 2 * (out0 + m * ls) - first;
-    if (p >= 0) lin[p + run(p)] = x[m].x;
-    if (p + 1 >= 0) lin[p + 1 + run(p + 1)] = x[m].y;
+    const double pc1 = fma(pc, fb.step1_c, -ps * fb.step1_s), ps1 = fma(pc, fb.step1_s, ps * fb.step1_c);
+    if (p >= 0) {
+      double v = x[m].x;
+      if (p < fb.limit) {
+        const double corr = fb.c0 + 2.0 * (fb.c1r * pc + fb.c1i * ps);
+        v += odd ? -corr : corr;
+      }
+      lin[p + run(p)] = v;
+    }
+    if (p + 1 >= 0) {
+      double v = x[m].y;
+      if (p + 1 < fb.limit) {
+        const double corr = fb.c0 + 2.0 * (fb.c1r * pc1 + fb.c1i * ps1);
+        v += odd ? corr : -corr;
+      }
+      lin[p + 1 + run(p + 1)] = v;
+    }
+    const double nc = fma(pc, fb.step512_c, -ps * fb.step512_s);
+    ps = fma(pc, fb.step512_s, ps * fb.step512_c);
+    pc = nc;
   }
   __syncthreads();
 }

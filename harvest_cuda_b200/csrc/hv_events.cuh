@@ -99,9 +99,11 @@ __device__ __forceinline__ double fine_edge(int64_t e, double s0, double s1) {
 // found by stepping forward while the next interval location is <= t. The four
 // tracks step in lockstep (one iteration advances every track that needs it)
 // so that their loads and divisions overlap; each track keeps the two edges
-// of its current right interval, so a step loads one edge. Every interval
-// location and value is computed with the reference's expressions, so the
-// results equal a binary search per frame bit for bit.
+// of its current right interval and the edge after them, loaded one step
+// ahead. Every interval location and value is computed with the reference's
+// expressions. interp1's slope factor (t - x0) / (x1 - x0) is taken as
+// (t - x0) times the interval's reciprocal width, formed once per interval:
+// within one rounding of the quotient.
 __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4], const int count[4],
                                          double centre, double* out, int frames) {
   const int nt = blockDim.x, tid = threadIdx.x;
@@ -150,6 +152,12 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
     y0[k] = fs / (ea[k] - em);
     y1[k] = fs / (eb[k] - ea[k]);
   }
+  double nxt[4], inv[4];   // the edge after eb; 1 / (x1 - x0)
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    nxt[k] = ev[k][imin(seg[k] + 2, count[k] - 1)];
+    inv[k] = 1.0 / (x1[k] - x0[k]);
+  }
   for (int f = fa; f < fb; ++f) {
     const double t = f * 1 / 1000.0;
     for (;;) {
@@ -160,9 +168,6 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
         any |= step[k];
       }
       if (!any) break;
-      double next[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) next[k] = step[k] ? ev[k][seg[k] + 2] : 0.0;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         if (!step[k]) continue;
@@ -170,15 +175,17 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
         x0[k] = x1[k];
         y0[k] = y1[k];
         ea[k] = eb[k];
-        eb[k] = next[k];
+        eb[k] = nxt[k];
+        nxt[k] = ev[k][imin(seg[k] + 2, count[k] - 1)];
         x1[k] = (ea[k] + eb[k]) / 2.0 / fs;
         y1[k] = fs / (eb[k] - ea[k]);
+        inv[k] = 1.0 / (x1[k] - x0[k]);
       }
     }
     double track[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      const double s = (t - x0[k]) / (x1[k] - x0[k]);
+      const double s = (t - x0[k]) * inv[k];
       track[k] = y0[k] + s * (y1[k] - y0[k]);
     }
     double val = (track[0] + track[1] + track[2] + track[3]) / 4.0;
