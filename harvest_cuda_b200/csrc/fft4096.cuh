@@ -160,16 +160,18 @@ __device__ __forceinline__ void inverse_last_pass_to_runs(double2* buf, const do
     sincospi(2.0 * static_cast<double>(r) / fb.n, &ps, &pc);
   }
   const bool odd = (fb.origin - first) & 1;   // parity of origin + p for even p (first is even)
+  // z = (c1r + i c1i) e^{-i phi} turns by e^{-i 2 pi / n} per sample; corr = c0 + 2 Re z.
+  double zr = fb.c1r * pc + fb.c1i * ps, zi = fb.c1i * pc - fb.c1r * ps;
   __syncthreads();
   double* lin = reinterpret_cast<double*>(buf);
 #pragma unroll
   for (int m = 0; m < 16; ++m) {
     const int p = 2 * (out0 + m * ls) - first;
-    const double pc1 = fma(pc, fb.step1_c, -ps * fb.step1_s), ps1 = fma(pc, fb.step1_s, ps * fb.step1_c);
+    const double zr1 = fma(fb.step1_c, zr, fb.step1_s * zi);
     if (p >= 0) {
       double v = x[m].x;
       if (p < fb.limit) {
-        const double corr = fb.c0 + 2.0 * (fb.c1r * pc + fb.c1i * ps);
+        const double corr = fma(2.0, zr, fb.c0);
         v += odd ? -corr : corr;
       }
       lin[p + run(p)] = v;
@@ -177,14 +179,14 @@ __device__ __forceinline__ void inverse_last_pass_to_runs(double2* buf, const do
     if (p + 1 >= 0) {
       double v = x[m].y;
       if (p + 1 < fb.limit) {
-        const double corr = fb.c0 + 2.0 * (fb.c1r * pc1 + fb.c1i * ps1);
+        const double corr = fma(2.0, zr1, fb.c0);
         v += odd ? corr : -corr;
       }
       lin[p + 1 + run(p + 1)] = v;
     }
-    const double nc = fma(pc, fb.step512_c, -ps * fb.step512_s);
-    ps = fma(pc, fb.step512_s, ps * fb.step512_c);
-    pc = nc;
+    const double nr = fma(fb.step512_c, zr, fb.step512_s * zi);
+    zi = fma(fb.step512_c, zi, -fb.step512_s * zr);
+    zr = nr;
   }
   __syncthreads();
 }
