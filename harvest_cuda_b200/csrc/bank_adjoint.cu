@@ -140,7 +140,7 @@ raw_adjoint(RawAdjointView v) {
         for (int k = 0; k < 4; ++k) {
           if (lo[k] >= hi[k]) continue;
           const int mid = (lo[k] + hi[k]) >> 1;
-          if ((edge[k][mid] + edge[k][mid + 1]) / 2.0 / fs <= t0) lo[k] = mid + 1; else hi[k] = mid;
+          if ((edge[k][mid] + edge[k][mid + 1]) * (0.5 / fs) <= t0) lo[k] = mid + 1; else hi[k] = mid;
           more |= lo[k] < hi[k];
         }
       }
@@ -151,8 +151,8 @@ raw_adjoint(RawAdjointView v) {
         ez[k] = e[-1];
         ea[k] = e[0];
         eb[k] = e[1];
-        x0[k] = (ez[k] + ea[k]) / 2.0 / fs;
-        x1[k] = (ea[k] + eb[k]) / 2.0 / fs;
+        x0[k] = (ez[k] + ea[k]) * (0.5 / fs);
+        x1[k] = (ea[k] + eb[k]) * (0.5 / fs);
         y0v[k] = fs / (ea[k] - ez[k]);
         y1v[k] = fs / (eb[k] - ea[k]);
       }
@@ -170,7 +170,7 @@ raw_adjoint(RawAdjointView v) {
             eb[k] = edge[k][seg[k] + 1];
             x0[k] = x1[k];
             y0v[k] = y1v[k];
-            x1[k] = (ea[k] + eb[k]) / 2.0 / fs;
+            x1[k] = (ea[k] + eb[k]) * (0.5 / fs);
             y1v[k] = fs / (eb[k] - ea[k]);
           }
           if (!any) break;

@@ -100,10 +100,13 @@ __device__ __forceinline__ double fine_edge(int64_t e, double s0, double s1) {
 // tracks step in lockstep (one iteration advances every track that needs it)
 // so that their loads and divisions overlap; each track keeps the two edges
 // of its current right interval and the edge after them, loaded one step
-// ahead. Every interval location and value is computed with the reference's
-// expressions. interp1's slope factor (t - x0) / (x1 - x0) is taken as
-// (t - x0) times the interval's reciprocal width, formed once per interval:
-// within one rounding of the quotient.
+// ahead. The reference's expressions are evaluated with fewer divisions,
+// each within a few roundings of its value: locations (e_j + e_{j+1}) (0.5 / fs),
+// and on a step, with the edges em < ea < eb of the two intervals and
+// r = 1 / ((eb - ea)(eb - em)), the value fs / (eb - ea) = fs (eb - em) r and
+// interp1's slope divisor 1 / (x1 - x0) = 2 fs / (eb - em) = 2 fs (eb - ea) r.
+// interp1 is continuous across intervals, so a location a rounding away
+// moves a frame's value by no more than that.
 __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4], const int count[4],
                                          double centre, double* out, int frames) {
   const int nt = blockDim.x, tid = threadIdx.x;
@@ -116,9 +119,11 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
   }
   if (fa >= fb) return;
   const double fs = B.fs_r;
+  const double half_rfs = 0.5 / fs, two_fs = 2.0 * fs;
   const double upper = centre * 1.1, lower = centre * 0.9;
   int seg[4], last[4];
   double x0[4], x1[4], y0[4], y1[4], ea[4], eb[4];   // ea, eb: edges seg, seg + 1
+  double inv[4];                                      // 1 / (x1 - x0)
   const double t0 = fa * 1 / 1000.0;
   // The first frame's segment of the four tracks, by binary searches
   // interleaved so that their dependent loads overlap.
@@ -135,7 +140,7 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
     for (int k = 0; k < 4; ++k) {
       if (lo[k] >= hi[k]) continue;
       const int mid = (lo[k] + hi[k]) >> 1;
-      if ((ev[k][mid] + ev[k][mid + 1]) / 2.0 / fs <= t0) lo[k] = mid + 1; else hi[k] = mid;
+      if ((ev[k][mid] + ev[k][mid + 1]) * half_rfs <= t0) lo[k] = mid + 1; else hi[k] = mid;
       more |= lo[k] < hi[k];
     }
   }
@@ -147,17 +152,15 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
     const double em = e[j - 1];
     ea[k] = e[j];
     eb[k] = e[j + 1];
-    x0[k] = (em + ea[k]) / 2.0 / fs;
-    x1[k] = (ea[k] + eb[k]) / 2.0 / fs;
+    x0[k] = (em + ea[k]) * half_rfs;
+    x1[k] = (ea[k] + eb[k]) * half_rfs;
     y0[k] = fs / (ea[k] - em);
     y1[k] = fs / (eb[k] - ea[k]);
+    inv[k] = two_fs / (eb[k] - em);
   }
-  double nxt[4], inv[4];   // the edge after eb; 1 / (x1 - x0)
+  double nxt[4];   // the edge after eb
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    nxt[k] = ev[k][imin(seg[k] + 2, count[k] - 1)];
-    inv[k] = 1.0 / (x1[k] - x0[k]);
-  }
+  for (int k = 0; k < 4; ++k) nxt[k] = ev[k][imin(seg[k] + 2, count[k] - 1)];
   for (int f = fa; f < fb; ++f) {
     const double t = f * 1 / 1000.0;
     for (;;) {
@@ -174,12 +177,15 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
         ++seg[k];
         x0[k] = x1[k];
         y0[k] = y1[k];
+        const double em = ea[k];
         ea[k] = eb[k];
         eb[k] = nxt[k];
         nxt[k] = ev[k][imin(seg[k] + 2, count[k] - 1)];
-        x1[k] = (ea[k] + eb[k]) / 2.0 / fs;
-        y1[k] = fs / (eb[k] - ea[k]);
-        inv[k] = 1.0 / (x1[k] - x0[k]);
+        x1[k] = (ea[k] + eb[k]) * half_rfs;
+        const double dl = eb[k] - ea[k], dw = eb[k] - em;
+        const double r = 1.0 / (dl * dw);
+        y1[k] = fs * dw * r;
+        inv[k] = two_fs * dl * r;
       }
     }
     double track[4];
