@@ -1,4 +1,6 @@
 // a10 and a13: channel aggregation, pruning and the best candidate per frame.
+#include <algorithm>
+
 #include "hv_stages.cuh"
 
 namespace hv {
@@ -36,14 +38,19 @@ __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
 // a13: RemoveUnreliableCandidates(Sub) with SelectBestF0 (harvest.cpp:636-688)
 // and SearchF0Base (harvest.cpp:693-705). One warp per frame: lanes take
 // columns, neighbour rows are read from the unpruned arrays, and the best
-// candidate is the first column holding the highest pruned score.
+// candidate is the first column holding the highest pruned score. The warp
+// first packs the nonzero candidates of the two neighbour rows into shared
+// memory (2 capacity doubles per warp), so each column's two minima run
+// over those only: a zero candidate c gives |ref - c| / ref = 1 for
+// ref > 0, which the error's cap at 1 already covers.
 __global__ void __launch_bounds__(128)
 prune_frames(BatchView v, const double* __restrict__ refined, const double* __restrict__ scores,
              const int* __restrict__ count, int64_t total_frames, double* __restrict__ pruned,
              double* __restrict__ pruned_scores, double* __restrict__ best) {
+  extern __shared__ double s_rows[];
   const int lane = threadIdx.x & 31;
   const int64_t gf = blockIdx.x * (int64_t)(blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (gf >= total_frames) return;
+  if (gf >= total_frames) return;   // uniform per warp
   const int c = owner(v.frame_off, v.clips, gf);
   const int64_t row0 = v.frame_off[c];
   const int frames = static_cast<int>(v.frame_off[c + 1] - row0);
@@ -52,22 +59,36 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
   const int cap = v.capacity;
   const double* row = refined + gf * cap;
   const bool interior = f >= 1 && f <= frames - 2;
+  double* s_next = s_rows + (threadIdx.x >> 5) * 2 * cap;
+  double* s_prev = s_next + cap;
+  int n_next = 0, n_prev = 0;
+  if (interior) {
+    const unsigned below = (1u << lane) - 1u;
+    for (int base = 0; base < columns; base += 32) {
+      const int j = base + lane;
+      const double a = j < columns ? row[cap + j] : 0.0;
+      const double b = j < columns ? row[j - cap] : 0.0;
+      const unsigned ma = __ballot_sync(0xffffffffu, a != 0.0), mb = __ballot_sync(0xffffffffu, b != 0.0);
+      if (a != 0.0) s_next[n_next + __popc(ma & below)] = a;
+      if (b != 0.0) s_prev[n_prev + __popc(mb & below)] = b;
+      n_next += __popc(ma);
+      n_prev += __popc(mb);
+    }
+    __syncwarp();
+  }
   double top = 0.0, pick = 0.0;
   int top_col = cap;
   for (int col = lane; col < cap; col += 32) {
     double ref = row[col], sc = scores[gf * cap + col];
     if (col < columns && interior && ref != 0) {
-      const double* next = row + cap;
-      const double* prev = row - cap;
       // SelectBestF0 leaves min(1, min_j |ref - c_j| / ref) as the error.
       // Correctly rounded division by the same positive ref is monotone, so
       // that equals the quotient of the smallest difference: one division
-      // per neighbour row, bit-identical.
-      double d1 = fabs(ref - next[0]), d2 = fabs(ref - prev[0]);
-      for (int j = 1; j < columns; ++j) {
-        d1 = fmin(d1, fabs(ref - next[j]));
-        d2 = fmin(d2, fabs(ref - prev[j]));
-      }
+      // per neighbour row, bit-identical. With no nonzero neighbour the
+      // quotient is infinite and the cap gives 1.
+      double d1 = __longlong_as_double(0x7ff0000000000000ll), d2 = d1;
+      for (int j = 0; j < n_next; ++j) d1 = fmin(d1, fabs(ref - s_next[j]));
+      for (int j = 0; j < n_prev; ++j) d2 = fmin(d2, fabs(ref - s_prev[j]));
       double e1 = d1 / ref, e2 = d2 / ref;
       if (e1 > 1.0) e1 = 1.0;
       if (e2 > 1.0) e2 = 1.0;
@@ -98,8 +119,11 @@ cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t tot
 cudaError_t launch_prune(const BatchView& v, const double* refined, const double* scores,
                          const int* count, int64_t total_frames, double* pruned,
                          double* pruned_scores, double* best, cudaStream_t stream) {
-  const int warps = 4;
-  prune_frames<<<static_cast<unsigned>((total_frames + warps - 1) / warps), 32 * warps, 0, stream>>>(
+  // Up to 4 warps per block, each with 2 capacity doubles of shared memory,
+  // within the default 48 KB (capacity < 1024).
+  const size_t per_warp = 2 * sizeof(double) * static_cast<size_t>(v.capacity);
+  const int warps = static_cast<int>(std::max<size_t>(1, std::min<size_t>(4, 49152 / per_warp)));
+  prune_frames<<<static_cast<unsigned>((total_frames + warps - 1) / warps), 32 * warps, warps * per_warp, stream>>>(
       v, refined, scores, count, total_frames, pruned, pruned_scores, best);
   return cudaGetLastError();
 }
