@@ -109,3 +109,15 @@ def test_batch_argument_validation():
         hv.harvest_batch(x, [0], 24000)
     with pytest.raises(TypeError):
         hv.harvest_batch(x.astype(np.float32), [0, 4800], 24000)
+
+
+def test_batch_pipeline_validates_arguments_before_needing_a_gpu():
+    from harvest_cuda_b200.pipeline import BatchPipeline
+    with pytest.raises(TypeError):
+        BatchPipeline(16000.0)
+    with pytest.raises(ValueError):
+        BatchPipeline(16000, depth=1)
+    import torch
+    if not torch.cuda.is_available():
+        with pytest.raises(RuntimeError, match="CUDA"):
+            BatchPipeline(16000)
