@@ -9,7 +9,9 @@ namespace hv {
 // thread per frame walks the bands: runs of at least 10 voiced channels
 // (first and last channel forced unvoiced) become one candidate, their mean
 // summed in channel order. `cand` is [frame][per_group]; per-clip maxima go
-// to count[] (zeroed by the caller).
+// to count[] (zeroed by the caller). Bands are loaded 8 at a time (the loads
+// of a group are independent), and each run's sum is carried along the walk:
+// the same additions, from 0, in channel order, as the reference's loop.
 __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
                                     int64_t total_frames, double* __restrict__ cand,
                                     int* __restrict__ count) {
@@ -17,17 +19,30 @@ __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
   if (gf >= total_frames) return;
   double* row = cand + gf * v.per_group;
   int found = 0, start = 0, prev = 0;
-  for (int b = 1; b < v.bands; ++b) {
-    int now = (b == v.bands - 1) ? 0 : (raw[b * total_frames + gf] > 0 ? 1 : 0);
-    if (now - prev == 1) start = b;
-    if (now - prev == -1 && b - start >= 10) {
-      double sum = 0.0;
-      for (int j = start; j < b; ++j) sum += raw[j * total_frames + gf];
-      sum /= (b - start);
-      if (found < v.per_group) row[found] = sum;
-      ++found;
+  double run = 0.0;
+  for (int b0 = 1; b0 < v.bands; b0 += 8) {
+    double r[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int b = b0 + u;
+      r[u] = b < v.bands - 1 ? raw[b * total_frames + gf] : 0.0;
     }
-    prev = now;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int b = b0 + u;
+      if (b >= v.bands) break;
+      const int now = (b == v.bands - 1) ? 0 : (r[u] > 0 ? 1 : 0);
+      if (now - prev == 1) {
+        start = b;
+        run = 0.0;
+      }
+      if (now - prev == -1 && b - start >= 10) {
+        if (found < v.per_group) row[found] = run / (b - start);
+        ++found;
+      }
+      if (now) run += r[u];
+      prev = now;
+    }
   }
   for (int j = found; j < v.per_group; ++j) row[j] = 0.0;
   // At most (bands - 1) / 11 runs fit, fewer than per_group; the clamp only
@@ -79,7 +94,8 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
   double top = 0.0, pick = 0.0;
   int top_col = cap;
   for (int col = lane; col < cap; col += 32) {
-    double ref = row[col], sc = scores[gf * cap + col];
+    // Columns from 7 count on hold no candidate (refinement zeroes them).
+    double ref = col < columns ? row[col] : 0.0, sc = col < columns ? scores[gf * cap + col] : 0.0;
     if (col < columns && interior && ref != 0) {
       // SelectBestF0 leaves min(1, min_j |ref - c_j| / ref) as the error.
       // Correctly rounded division by the same positive ref is monotone, so

@@ -257,8 +257,10 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
   };
   double nc, ns;
   phase(0, nc, ns);
+  // Blackman window 0.42 + 0.5 cos + 0.08 cos 2 as 0.34 + 0.5 cos + 0.16 cos^2.
+  auto blackman = [](double c) { return fma(fma(0.16, c, 0.5), c, 0.34); };
   double w_prev = 0.0;
-  double w_cur = 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0);
+  double w_cur = blackman(nc);
   const bool inside = cw.base - 1 >= 0 && cw.base - 1 + len <= y_len;
   const double* yb = y + (cw.base - 1);
   auto accumulate = [&](int i, double w, double dw) {
@@ -280,8 +282,8 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
     const int i1 = imin(i0 + kAnchor, len - 1);
 #pragma unroll 2
     for (int i = i0; i < i1; ++i) {
-      const double w_next = 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0);
-      accumulate(i, w_cur, -(w_next - w_prev) / 2.0);
+      const double w_next = blackman(nc);
+      accumulate(i, w_cur, w_prev - w_next);
       const double rc = fma(nc, dc, -ns * ds);
       ns = fma(nc, ds, ns * dc);
       nc = rc;
@@ -289,7 +291,7 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
       w_cur = w_next;
     }
   }
-  accumulate(len - 1, w_cur, -(0.0 - w_prev) / 2.0);
+  accumulate(len - 1, w_cur, w_prev);
 #pragma unroll
   for (int h = 0; h < 6; ++h) {
     const double2 step = bin_twiddle(tw, cw.bin[h], n);                        // e^{-i theta}
@@ -300,12 +302,12 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
     double re = a1[h] - ct * s2, im = st * s2;
     sp.mr[h] = re * cp - im * sp_;
     sp.mi[h] = re * sp_ + im * cp;
-    // d sequence
+    // d sequence, accumulated with twice the difference window
     s2 = d2[h];
     re = d1[h] - ct * s2;
     im = st * s2;
-    sp.dr[h] = re * cp - im * sp_;
-    sp.di[h] = re * sp_ + im * cp;
+    sp.dr[h] = 0.5 * (re * cp - im * sp_);
+    sp.di[h] = 0.5 * (re * sp_ + im * cp);
   }
 }
 
