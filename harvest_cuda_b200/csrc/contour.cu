@@ -83,6 +83,76 @@ __device__ __forceinline__ double warp_select_best(double ref, const double* can
   return best_v;
 }
 
+// A candidate row held in registers, column lane + 32 k in slot k, for
+// rows of at most kRowSlots * 32 columns; loading the next frame's row
+// before selecting in the current one hides its latency.
+constexpr int kRowSlots = 8;
+struct CandRow {
+  double c[kRowSlots];
+  __device__ __forceinline__ void load(const double* cand, int count) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < kRowSlots; ++k) c[k] = lane + 32 * k < count ? cand[lane + 32 * k] : 0.0;
+  }
+};
+
+// warp_select_best on a row in registers: the same columns in the same order
+// per lane and the same reduction, so the same candidate.
+__device__ __forceinline__ double warp_select_best(double ref, const CandRow& row, int count, double allowed) {
+  const int lane = threadIdx.x & 31;
+  double best_e = allowed, best_v = 0.0;
+  int best_i = -1;
+#pragma unroll
+  for (int k = 0; k < kRowSlots; ++k) {
+    const int i = lane + 32 * k;
+    if (i >= count) break;
+    const double c = row.c[k];
+    const double e = fabs(ref - c) / ref;
+    if (e <= best_e) { best_e = e; best_i = i; best_v = c; }
+  }
+  for (int o = 16; o; o >>= 1) {
+    const double oe = __shfl_xor_sync(kAll, best_e, o), ov = __shfl_xor_sync(kAll, best_v, o);
+    const int oi = __shfl_xor_sync(kAll, best_i, o);
+    if (oi >= 0 && (best_i < 0 || oe < best_e || (oe == best_e && oi > best_i))) {
+      best_e = oe; best_i = oi; best_v = ov;
+    }
+  }
+  return best_v;
+}
+
+// One direction of ExtendF0 (harvest.cpp:791-824) from frame `from` with
+// value `cur`: frames from + dir, from + 2 dir, ... up to `steps` of them,
+// each SelectBestF0 against the last accepted value, stopping after four
+// misses in a row. Values go to out[k] (lane 0); returns the last frame
+// that took a value.
+__device__ __forceinline__ int extend_f0(const double* cand, int64_t stride, int columns, int from, int dir,
+                                         int steps, double cur, double* out) {
+  const int lane = threadIdx.x & 31;
+  int reached = from, misses = 0;
+  if (columns <= kRowSlots * 32) {
+    CandRow row, next;
+    if (steps > 0) row.load(cand + static_cast<int64_t>(from + dir) * stride, columns);
+    for (int k = 0; k < steps; ++k) {
+      const int idx = from + dir * (k + 1);
+      if (k + 1 < steps) next.load(cand + static_cast<int64_t>(idx + dir) * stride, columns);
+      const double val = warp_select_best(cur, row, columns, 0.18);
+      if (lane == 0) out[k] = val;
+      if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
+      if (misses == 4) break;
+      row = next;
+    }
+  } else {
+    for (int k = 0; k < steps; ++k) {
+      const int idx = from + dir * (k + 1);
+      const double val = warp_select_best(cur, cand + static_cast<int64_t>(idx) * stride, columns, 0.18);
+      if (lane == 0) out[k] = val;
+      if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
+      if (misses == 4) break;
+    }
+  }
+  return reached;
+}
+
 // SearchScore (harvest.cpp:901-907).
 __device__ __forceinline__ double search_score(double f0, const double* cand, const double* score,
                                                int count) {
@@ -197,6 +267,87 @@ __device__ bool smooth_section(P padded, int st, int ed, int64_t len, double* ou
   return true;
 }
 
+// Sections at least this long are smoothed by the whole warp.
+constexpr int kLongSection = 2048;
+// Steps a lane runs from a zero state before its chunk: the filter's poles
+// have radius sqrt(0.766) = 0.875, so a state's influence falls below
+// 0.875^512 (1e-30) of it.
+constexpr int kWarm = 512;
+
+// smooth_section for a long section [st, ed], by the whole warp. The held
+// head and tail run as in smooth_section (every lane computes the head's
+// constant-input steps; lane 0 runs the tail and its checkpointed backward
+// pass in `tail`, cap doubles). The body, forward and then backward, is cut
+// into 32 chunks, one per lane; a lane starts kWarm steps before its chunk
+// from a zero state, or from the exact state where that reaches the end of
+// the body. Its chunk's outputs then differ from a single pass's only by
+// rounding (a few units in the last place).
+template <class P>
+__device__ void smooth_section_warp(P padded, int st, int ed, int64_t len, double* out, double* tail,
+                                    int64_t cap) {
+  const int lag = 300, lane = threadIdx.x & 31;
+  const double head = padded(st), tail_value = padded(ed);
+  const int n = ed - st + 1, chunk = (n + 31) / 32;
+  const int c0 = imin(st + lane * chunk, ed + 1), c1 = imin(c0 + chunk, ed + 1);   // this lane's [c0, c1)
+  // Forward body.
+  Butter fw;
+  int j = c0 - kWarm;
+  if (j <= st) {
+    fw.run_constant(head, st);
+    j = st;
+  }
+  for (; j < c0; ++j) fw.step(padded(j));
+  for (; j < c1; ++j) out[j - lag] = fw.step(padded(j));
+  __syncwarp();                        // forward outputs visible to every lane
+  const int owner = (n - 1) / chunk;   // lane whose chunk ends at ed
+  fw.w0 = __shfl_sync(kAll, fw.w0, owner);
+  fw.w1 = __shfl_sync(kAll, fw.w1, owner);
+  // Held tail, forward and backward, on lane 0 (as in smooth_section).
+  Butter bw;
+  if (lane == 0) {
+    const int64_t trailing = len - 1 - ed;
+    const int64_t stretch = cap / 2;
+    double* saved = tail + stretch;
+    int64_t stored = 0;
+    double settled = 0.0;
+    bool fixed = false;
+    for (int64_t k = 0; k < trailing; ++k) {
+      if (stored % stretch == 0) {
+        const int64_t c = stored / stretch;
+        saved[2 * c] = fw.w0;
+        saved[2 * c + 1] = fw.w1;
+      }
+      double p0 = fw.w0, p1 = fw.w1;
+      double o = fw.step(tail_value);
+      if (fw.w0 == p0 && fw.w1 == p1) { settled = o; fixed = true; break; }
+      ++stored;
+    }
+    if (fixed) bw.run_constant(settled, trailing - stored);
+    for (int64_t first = (stored > 0 ? (stored - 1) / stretch : -1) * stretch; first >= 0; first -= stretch) {
+      const int64_t m = stored - first < stretch ? stored - first : stretch;
+      Butter re;
+      re.w0 = saved[2 * (first / stretch)];
+      re.w1 = saved[2 * (first / stretch) + 1];
+      for (int64_t k = 0; k < m; ++k) tail[k] = re.step(tail_value);
+      for (int64_t k = m - 1; k >= 0; --k) bw.step(tail[k]);
+    }
+  }
+  const double t0 = __shfl_sync(kAll, bw.w0, 0), t1 = __shfl_sync(kAll, bw.w1, 0);
+  // Backward body: every lane first runs its warm-up over forward outputs of
+  // later chunks, then (after all have) overwrites its own chunk.
+  Butter b;
+  j = c1 - 1 + kWarm;
+  if (j >= ed) {
+    b.w0 = t0;
+    b.w1 = t1;
+    j = ed;
+  }
+  for (; j >= c1; --j) b.step(out[j - lag]);
+  __syncwarp();
+  for (; j >= c0; --j) out[j - lag] = b.step(out[j - lag]);
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
   const int c = blockIdx.x;
   const int lane = threadIdx.x;
@@ -253,29 +404,11 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
     for (int k = lane; k < kExtend; k += 32) fwd[k] = bwd[k] = 0.0;
     __syncwarp();
     {  // ExtendF0 forward from the end (harvest.cpp:867-870)
-      const int last = imin(F - 2, ed + 100);
-      double cur = s2[ed];
-      int reached = ed, misses = 0;
-      for (int k = 0; k <= last - ed; ++k) {
-        const int idx = ed + k + 1;
-        const double val = warp_select_best(cur, cand + static_cast<int64_t>(idx) * stride, columns, 0.18);
-        if (lane == 0) fwd[k] = val;
-        if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
-        if (misses == 4) break;
-      }
+      const int reached = extend_f0(cand, stride, columns, ed, 1, imin(F - 2, ed + 100) - ed + 1, s2[ed], fwd);
       if (lane == 0) sec[8 * i + 3] = reached;
     }
     {  // ExtendF0 backward from the start (harvest.cpp:871-873)
-      const int last = imax(1, st - 100);
-      double cur = s2[st];
-      int reached = st, misses = 0;
-      for (int k = 0; k <= st - last; ++k) {
-        const int idx = st - k - 1;
-        const double val = warp_select_best(cur, cand + static_cast<int64_t>(idx) * stride, columns, 0.18);
-        if (lane == 0) bwd[k] = val;
-        if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
-        if (misses == 4) break;
-      }
+      const int reached = extend_f0(cand, stride, columns, st, -1, st - imax(1, st - 100) + 1, s2[st], bwd);
       if (lane == 0) sec[8 * i + 2] = reached;
     }
     if (lane == 0) {
@@ -404,6 +537,7 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
   if (lane == 0) deferred_count = 0;
   __syncwarp();
   for (int s = lane; s < nbs / 2; s += 32) {
+    if (bl[2 * s + 1] - bl[2 * s] + 1 >= kLongSection) continue;
     if (!smooth_section(padded, bl[2 * s], bl[2 * s + 1], len, sm, tails + lane * kTransient, kTransient))
       deferred[atomicAdd(&deferred_count, 1)] = s;
   }
@@ -416,6 +550,10 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
       smooth_section(padded, bl[2 * s], bl[2 * s + 1], len, sm, shared_tail, len);
     }
   __syncwarp();
+  // Long sections, one at a time with the whole warp.
+  for (int s = 0; s < nbs / 2; ++s)
+    if (bl[2 * s + 1] - bl[2 * s] + 1 >= kLongSection)
+      smooth_section_warp(padded, bl[2 * s], bl[2 * s + 1], len, sm, shared_tail, len);
   // Resampling (harvest.cpp:1246-1251); for frame_period 1 the same
   // expression reproduces the direct branch (harvest.cpp:1230-1235).
   const int64_t o0 = v.out_off[c];
