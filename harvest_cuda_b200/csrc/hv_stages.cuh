@@ -159,6 +159,7 @@ struct RefineBuffers {
   int* total;          // [1]
   RefineJob* jobs;     // [frames * capacity]
   ulonglong2* keys;    // [frames * per_group] refinement key of every official candidate
+  unsigned long long* leaders;  // [frames * per_group] job classes of the 7 overlap cells, 1 byte each
   const double2* twiddles;  // [kTwiddleN] e^{-2 pi i t / kTwiddleN}
 };
 // Launch shape of the refinement jobs: minimum resident 128-thread blocks per

@@ -90,44 +90,60 @@ __global__ void candidate_keys(BatchView v, const double* __restrict__ cand, int
 // column j (groups g = 0..6) at this frame. A cell is a job when its
 // candidate is nonzero and no lower group of the same j holds a candidate
 // with the same key; the leader's job also serves those later siblings.
-// Pass 1 (kScatter = false) counts jobs per window-length class, pass 2
-// writes them at the class offsets.
+// Pass 1 (kScatter = false) finds the jobs, counts them per window-length
+// class and records each cell's class + 1 (0: no job) in a byte of
+// leaders[item]; pass 2 reads that record and writes the jobs at the class
+// offsets.
 template <bool kScatter>
 __global__ void __launch_bounds__(256)
 refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
-              const ulonglong2* __restrict__ keys, int64_t total_frames, int* __restrict__ class_count,
-              int* __restrict__ class_cursor, RefineJob* __restrict__ jobs) {
+              const ulonglong2* __restrict__ keys, int64_t total_frames, unsigned long long* __restrict__ leaders,
+              int* __restrict__ class_count, int* __restrict__ class_cursor, RefineJob* __restrict__ jobs) {
   __shared__ int s_count[kRefineClasses], s_base[kRefineClasses];
   for (int i = threadIdx.x; i < kRefineClasses; i += blockDim.x) s_count[i] = 0;
   __syncthreads();
   const int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const bool valid = item < total_frames * v.per_group;
   int cls[7], rank[7];
-  double f0[7];
-  int64_t gf = 0;
-  int K = 0, j = 0;
 #pragma unroll
   for (int g = 0; g < 7; ++g) cls[g] = -1;
-  if (item < total_frames * v.per_group) {
-    gf = item / v.per_group;
-    j = static_cast<int>(item - gf * v.per_group);
-    const int c = owner(v.frame_off, v.clips, gf);
-    K = count[c];
-    if (j < K) {
-      const int64_t row0 = v.frame_off[c];
-      const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
-      ulonglong2 key[7];
+  if (valid) {
+    if (!kScatter) {
+      const int64_t gf = item / v.per_group;
+      const int j = static_cast<int>(item - gf * v.per_group);
+      const int c = owner(v.frame_off, v.clips, gf);
+      const int K = count[c];
+      unsigned long long record = 0;
+      if (j < K) {
+        const int64_t row0 = v.frame_off[c];
+        const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
+        ulonglong2 key[7];
+        bool live[7];
+#pragma unroll
+        for (int g = 0; g < 7; ++g) {
+          const int64_t slot = sibling_slot(v, row0, frames, f, g, j);
+          live[g] = slot >= 0 && cand[slot] > 0.0;
+          key[g] = live[g] ? keys[slot] : make_ulonglong2(0ull, 0ull);
+          bool leader = live[g];
+#pragma unroll
+          for (int g2 = 0; g2 < g; ++g2)
+            if (live[g2] && same_key(key[g], key[g2])) leader = false;
+          if (leader) {
+            const int half = static_cast<int>(key[g].x >> 32);
+            cls[g] = imin(size_class(2 * half + 1), kRefineClasses - 1);
+            rank[g] = atomicAdd(&s_count[cls[g]], 1);
+            record |= static_cast<unsigned long long>(cls[g] + 1) << (8 * g);
+          }
+        }
+      }
+      leaders[item] = record;
+    } else {
+      const unsigned long long record = leaders[item];
 #pragma unroll
       for (int g = 0; g < 7; ++g) {
-        const int64_t slot = sibling_slot(v, row0, frames, f, g, j);
-        f0[g] = slot >= 0 ? cand[slot] : 0.0;
-        key[g] = f0[g] > 0.0 ? keys[slot] : make_ulonglong2(0ull, 0ull);
-        bool leader = f0[g] > 0.0;
-#pragma unroll
-        for (int g2 = 0; g2 < g; ++g2)
-          if (f0[g2] > 0.0 && same_key(key[g], key[g2])) leader = false;
-        if (leader) {
-          const int half = static_cast<int>(key[g].x >> 32);
-          cls[g] = imin(size_class(2 * half + 1), kRefineClasses - 1);
+        const int b = static_cast<int>((record >> (8 * g)) & 0xff);
+        if (b) {
+          cls[g] = b - 1;
           rank[g] = atomicAdd(&s_count[cls[g]], 1);
         }
       }
@@ -139,13 +155,23 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
     if (kScatter) s_base[i] = atomicAdd(&class_cursor[i], s_count[i]);
     else atomicAdd(&class_count[i], s_count[i]);
   }
-  if (!kScatter) return;
+  if (!kScatter || !valid) return;
   __syncthreads();
+  bool any = false;
+#pragma unroll
+  for (int g = 0; g < 7; ++g) any |= cls[g] >= 0;
+  if (!any) return;
+  const int64_t gf = item / v.per_group;
+  const int j = static_cast<int>(item - gf * v.per_group);
+  const int c = owner(v.frame_off, v.clips, gf);
+  const int K = count[c];
+  const int64_t row0 = v.frame_off[c];
+  const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
 #pragma unroll
   for (int g = 0; g < 7; ++g) {
     if (cls[g] < 0) continue;
     RefineJob job;
-    job.f0c = f0[g];
+    job.f0c = cand[sibling_slot(v, row0, frames, f, g, j)];
     job.key = gf * kRefineColumns + g * K + j;
     jobs[s_base[cls[g]] + rank[g]] = job;
   }
@@ -471,10 +497,10 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
   const int64_t slots = total_frames * v.per_group;
   const unsigned grid = static_cast<unsigned>((slots + 255) / 256);
   candidate_keys<<<grid, 256, 0, stream>>>(v, cand, slots, b.keys);
-  refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.class_count,
+  refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.leaders, b.class_count,
                                                  b.class_cursor, b.jobs);
   refine_offsets<<<1, 32, 0, stream>>>(b.class_count, b.class_cursor, b.total);
-  refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.class_count,
+  refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.leaders, b.class_count,
                                                 b.class_cursor, b.jobs);
   const unsigned job_grid = static_cast<unsigned>(sms * shape.blocks_per_sm);
   auto kernel = shape.min_blocks == 4 ? refine_jobs<4> : (shape.min_blocks == 5 ? refine_jobs<5> : refine_jobs<1>);
