@@ -91,14 +91,17 @@ __global__ void candidate_keys(BatchView v, const double* __restrict__ cand, int
 // candidate is nonzero and no lower group of the same j holds a candidate
 // with the same key; the leader's job also serves those later siblings.
 // Pass 1 (kScatter = false) finds the jobs, counts them per window-length
-// class and records each cell's class + 1 (0: no job) in a byte of
-// leaders[item]; pass 2 reads that record and writes the jobs at the class
-// offsets.
+// class, records each cell's class + 1 (0: no job) in a byte of
+// leaders[item] and zeroes the refined F0 and score of cells without a
+// candidate (cells of later siblings are written by their leader's job);
+// pass 2 reads the record and writes the jobs at the class offsets. Columns
+// from 7 count on are left as they are: nothing reads them.
 template <bool kScatter>
 __global__ void __launch_bounds__(256)
 refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
               const ulonglong2* __restrict__ keys, int64_t total_frames, unsigned long long* __restrict__ leaders,
-              int* __restrict__ class_count, int* __restrict__ class_cursor, RefineJob* __restrict__ jobs) {
+              int* __restrict__ class_count, int* __restrict__ class_cursor, RefineJob* __restrict__ jobs,
+              double* __restrict__ refined, double* __restrict__ scores) {
   __shared__ int s_count[kRefineClasses], s_base[kRefineClasses];
   for (int i = threadIdx.x; i < kRefineClasses; i += blockDim.x) s_count[i] = 0;
   __syncthreads();
@@ -123,6 +126,10 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
         for (int g = 0; g < 7; ++g) {
           const int64_t slot = sibling_slot(v, row0, frames, f, g, j);
           live[g] = slot >= 0 && cand[slot] > 0.0;
+          if (!live[g]) {
+            refined[gf * v.capacity + g * K + j] = 0.0;
+            scores[gf * v.capacity + g * K + j] = 0.0;
+          }
           key[g] = live[g] ? keys[slot] : make_ulonglong2(0ull, 0ull);
           bool leader = live[g];
 #pragma unroll
@@ -489,19 +496,16 @@ refine_adjoint(BatchView v, const double* __restrict__ y, const double* __restri
 cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const double* y,
                           const double* cand, const int* count, int64_t total_frames, double* refined,
                           double* scores, int sms, RefineShape shape, cudaStream_t stream) {
-  const int64_t cells = total_frames * v.capacity;
   cudaError_t e;
   if ((e = cudaMemsetAsync(b.class_count, 0, sizeof(int) * kRefineClasses, stream)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(refined, 0, sizeof(double) * cells, stream)) != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(scores, 0, sizeof(double) * cells, stream)) != cudaSuccess) return e;
   const int64_t slots = total_frames * v.per_group;
   const unsigned grid = static_cast<unsigned>((slots + 255) / 256);
   candidate_keys<<<grid, 256, 0, stream>>>(v, cand, slots, b.keys);
   refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.leaders, b.class_count,
-                                                 b.class_cursor, b.jobs);
+                                                 b.class_cursor, b.jobs, refined, scores);
   refine_offsets<<<1, 32, 0, stream>>>(b.class_count, b.class_cursor, b.total);
   refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.leaders, b.class_count,
-                                                b.class_cursor, b.jobs);
+                                                b.class_cursor, b.jobs, refined, scores);
   const unsigned job_grid = static_cast<unsigned>(sms * shape.blocks_per_sm);
   auto kernel = shape.min_blocks == 4 ? refine_jobs<4> : (shape.min_blocks == 5 ? refine_jobs<5> : refine_jobs<1>);
   kernel<<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, cand, count, b.keys, b.twiddles, refined, scores);
