@@ -93,10 +93,11 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
   }
   double top = 0.0, pick = 0.0;
   int top_col = cap;
-  for (int col = lane; col < cap; col += 32) {
-    // Columns from 7 count on hold no candidate (refinement zeroes them).
-    double ref = col < columns ? row[col] : 0.0, sc = col < columns ? scores[gf * cap + col] : 0.0;
-    if (col < columns && interior && ref != 0) {
+  // Columns from 7 count on hold no candidate; they are neither read nor
+  // written (every reader stops at 7 count).
+  for (int col = lane; col < columns; col += 32) {
+    double ref = row[col], sc = scores[gf * cap + col];
+    if (interior && ref != 0) {
       // SelectBestF0 leaves min(1, min_j |ref - c_j| / ref) as the error.
       // Correctly rounded division by the same positive ref is monotone, so
       // that equals the quotient of the smallest difference: one division
@@ -113,7 +114,7 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
     }
     pruned[gf * cap + col] = ref;
     pruned_scores[gf * cap + col] = sc;
-    if (col < columns && sc > top) { top = sc; pick = ref; top_col = col; }
+    if (sc > top) { top = sc; pick = ref; top_col = col; }
   }
   for (int o = 16; o; o >>= 1) {
     double ot = __shfl_down_sync(0xffffffffu, top, o);

@@ -1440,11 +1440,11 @@ int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor, doubl
     int64_t offsets[2] = {0, n};
     Plan& p = ws.prepare(Settings{fs, f0_floor, f0_ceil, 5.0}, offsets, 1, ws.stream);
     check(cudaMemcpyAsync(ws.ptr<double>(p.at.x), x, 8 * n, cudaMemcpyHostToDevice, ws.stream), "cudaMemcpy(x)");
-    // The refinement leaves the columns past 7 count untouched; the dump
-    // shows them as zeros.
+    // Refinement and pruning leave the columns past 7 count untouched; the
+    // dump shows them as zeros.
     const int64_t F = p.frame_off[1];
-    check(cudaMemsetAsync(ws.ptr<double>(p.at.refined), 0, 8 * size_t(p.capacity) * F, ws.stream), "memset");
-    check(cudaMemsetAsync(ws.ptr<double>(p.at.scores), 0, 8 * size_t(p.capacity) * F, ws.stream), "memset");
+    for (size_t at : {p.at.refined, p.at.scores, p.at.pruned, p.at.pruned_scores})
+      check(cudaMemsetAsync(ws.ptr<double>(at), 0, 8 * size_t(p.capacity) * F, ws.stream), "memset");
     ws.run(p, ws.stream, false, false);
     auto out = [&](void* dst, size_t at, size_t bytes) {
       if (dst) check(cudaMemcpyAsync(dst, ws.ptr<char>(at), bytes, cudaMemcpyDeviceToHost, ws.stream), "cudaMemcpy");
