@@ -67,19 +67,35 @@ __global__ void decimate_segment_states(DecimateView v, const double* __restrict
 }
 
 // Chains zero-state segment results into true initial states, in place:
-// on return states[seg] holds the state entering the segment.
+// on return states[seg] holds the state entering the segment. One thread
+// per clip; the zero-state results of 8 segments are loaded before they are
+// chained, so the chain waits for memory once per 8 segments.
 __global__ void decimate_chain(DecimateView v, double* __restrict__ states) {
+  constexpr int kAhead = 8;
   int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= v.clips) return;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
-  for (int64_t seg = v.seg_off[c]; seg < v.seg_off[c + 1]; ++seg) {
-    double z0 = states[3 * seg], z1 = states[3 * seg + 1], z2 = states[3 * seg + 2];
-    states[3 * seg] = s0; states[3 * seg + 1] = s1; states[3 * seg + 2] = s2;
-    const double* m = v.trans;
-    double n0 = m[0] * s0 + m[1] * s1 + m[2] * s2 + z0;
-    double n1 = m[3] * s0 + m[4] * s1 + m[5] * s2 + z1;
-    double n2 = m[6] * s0 + m[7] * s1 + m[8] * s2 + z2;
-    s0 = n0; s1 = n1; s2 = n2;
+  const double* m = v.trans;
+  const int64_t end = v.seg_off[c + 1];
+  for (int64_t seg0 = v.seg_off[c]; seg0 < end; seg0 += kAhead) {
+    double z[3 * kAhead];
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k)
+      if (seg0 + k < end) {
+        z[3 * k] = states[3 * (seg0 + k)];
+        z[3 * k + 1] = states[3 * (seg0 + k) + 1];
+        z[3 * k + 2] = states[3 * (seg0 + k) + 2];
+      }
+#pragma unroll
+    for (int k = 0; k < kAhead; ++k) {
+      if (seg0 + k >= end) break;
+      const int64_t seg = seg0 + k;
+      states[3 * seg] = s0; states[3 * seg + 1] = s1; states[3 * seg + 2] = s2;
+      double n0 = m[0] * s0 + m[1] * s1 + m[2] * s2 + z[3 * k];
+      double n1 = m[3] * s0 + m[4] * s1 + m[5] * s2 + z[3 * k + 1];
+      double n2 = m[6] * s0 + m[7] * s1 + m[8] * s2 + z[3 * k + 2];
+      s0 = n0; s1 = n1; s2 = n2;
+    }
   }
 }
 
