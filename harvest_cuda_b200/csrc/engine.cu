@@ -641,6 +641,8 @@ struct Workspace {
     int items_n = static_cast<int>(p->items.size());
     p->bank_ctas = std::max(1, std::min(items_n, sms * per_sm));
     const int64_t F = p->frame_off[B];
+    if (F >= (int64_t(1) << kJobSiblingShift) / kRefineColumns)
+      throw InvalidArgument("batch too long: more than 2^31 analysis frames");
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t at = off; off = align_up(off + bytes); return at; };
     p->at.meta = take(p->meta.size());
@@ -660,7 +662,7 @@ struct Workspace {
     p->at.jobs = take(sizeof(RefineJob) * size_t(p->capacity) * F);
     p->at.classes = take(sizeof(int) * (2 * kRefineClasses + 1));
     p->at.keys = take(sizeof(ulonglong2) * size_t(p->per_group) * F);
-    p->at.leaders = take(sizeof(unsigned long long) * size_t(p->per_group) * F);
+    p->at.leaders = take(2 * sizeof(unsigned long long) * size_t(p->per_group) * F);
     p->at.refined = take(8 * size_t(p->capacity) * F);
     p->at.scores = take(8 * size_t(p->capacity) * F);
     p->at.pruned = take(8 * size_t(p->capacity) * F);

@@ -149,6 +149,9 @@ cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t tot
                               double* cand, int* count, cudaStream_t stream);
 constexpr int kRefineClasses = 72;   // quarter-octave window-length classes
 constexpr int kRefineColumns = 1024; // job key = frame * kRefineColumns + column
+// Bits 41-47 of a job key: the overlap groups whose cells share the job's
+// spectra (frame * kRefineColumns + column stays below 2^41).
+constexpr int kJobSiblingShift = 41;
 struct RefineJob {
   double f0c;
   long long key;
@@ -159,7 +162,7 @@ struct RefineBuffers {
   int* total;          // [1]
   RefineJob* jobs;     // [frames * capacity]
   ulonglong2* keys;    // [frames * per_group] refinement key of every official candidate
-  unsigned long long* leaders;  // [frames * per_group] job classes of the 7 overlap cells, 1 byte each
+  unsigned long long* leaders;  // [frames * per_group][2] job classes and sibling masks of the 7 overlap cells
   const double2* twiddles;  // [kTwiddleN] e^{-2 pi i t / kTwiddleN}
 };
 // Launch shape of the refinement jobs: minimum resident 128-thread blocks per

@@ -91,11 +91,13 @@ __global__ void candidate_keys(BatchView v, const double* __restrict__ cand, int
 // candidate is nonzero and no lower group of the same j holds a candidate
 // with the same key; the leader's job also serves those later siblings.
 // Pass 1 (kScatter = false) finds the jobs, counts them per window-length
-// class, records each cell's class + 1 (0: no job) in a byte of
-// leaders[item] and zeroes the refined F0 and score of cells without a
-// candidate (cells of later siblings are written by their leader's job);
-// pass 2 reads the record and writes the jobs at the class offsets. Columns
-// from 7 count on are left as they are: nothing reads them.
+// class, records each cell's class + 1 (0: no job) in byte g of
+// leaders[2 item] and each job's siblings (the later groups with the same
+// key) as bits g2 of the 7-bit field g of leaders[2 item + 1], and zeroes the
+// refined F0 and score of cells without a candidate (cells of siblings are
+// written by their leader's job); pass 2 reads the records and writes the
+// jobs at the class offsets, the sibling bits in the job key's bits 41-47.
+// Columns from 7 count on are left as they are: nothing reads them.
 template <bool kScatter>
 __global__ void __launch_bounds__(256)
 refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
@@ -116,7 +118,7 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
       const int j = static_cast<int>(item - gf * v.per_group);
       const int c = owner(v.frame_off, v.clips, gf);
       const int K = count[c];
-      unsigned long long record = 0;
+      unsigned long long record = 0, sibling_record = 0;
       if (j < K) {
         const int64_t row0 = v.frame_off[c];
         const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
@@ -142,10 +144,20 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
             record |= static_cast<unsigned long long>(cls[g] + 1) << (8 * g);
           }
         }
+#pragma unroll
+        for (int g = 0; g < 7; ++g) {
+          if (cls[g] < 0) continue;
+          unsigned long long m = 0;
+#pragma unroll
+          for (int g2 = g + 1; g2 < 7; ++g2)
+            if (live[g2] && same_key(key[g], key[g2])) m |= 1ull << g2;
+          sibling_record |= m << (7 * g);
+        }
       }
-      leaders[item] = record;
+      leaders[2 * item] = record;
+      leaders[2 * item + 1] = sibling_record;
     } else {
-      const unsigned long long record = leaders[item];
+      const unsigned long long record = leaders[2 * item];
 #pragma unroll
       for (int g = 0; g < 7; ++g) {
         const int b = static_cast<int>((record >> (8 * g)) & 0xff);
@@ -174,12 +186,14 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
   const int K = count[c];
   const int64_t row0 = v.frame_off[c];
   const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
+  const unsigned long long sibling_record = leaders[2 * item + 1];
 #pragma unroll
   for (int g = 0; g < 7; ++g) {
     if (cls[g] < 0) continue;
     RefineJob job;
     job.f0c = cand[sibling_slot(v, row0, frames, f, g, j)];
-    job.key = gf * kRefineColumns + g * K + j;
+    job.key = static_cast<long long>(gf * kRefineColumns + g * K + j) |
+              static_cast<long long>((sibling_record >> (7 * g)) & 0x7f) << kJobSiblingShift;
     jobs[s_base[cls[g]] + rank[g]] = job;
   }
 }
@@ -391,8 +405,10 @@ refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restri
   const int total_jobs = *total;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total_jobs; idx += gridDim.x * blockDim.x) {
     const RefineJob job = jobs[idx];
-    const int64_t gf = job.key / kRefineColumns;
-    const int col = static_cast<int>(job.key - gf * kRefineColumns);
+    const long long cell = job.key & ((1ll << kJobSiblingShift) - 1);
+    const unsigned siblings = static_cast<unsigned>(job.key >> kJobSiblingShift);
+    const int64_t gf = cell / kRefineColumns;
+    const int col = static_cast<int>(cell - gf * kRefineColumns);
     const int c = owner(v.frame_off, v.clips, gf);
     const int64_t row0 = v.frame_off[c];
     const int f = static_cast<int>(gf - row0);
@@ -410,12 +426,9 @@ refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restri
     scores[gf * v.capacity + col] = score;
     const int frames = static_cast<int>(v.frame_off[c + 1] - row0);
     const int K = count[c], g = col / K, j = col - g * K;
-    const ulonglong2 key = keys[sibling_slot(v, row0, frames, f, g, j)];
-    for (int g2 = g + 1; g2 < 7; ++g2) {
-      const int64_t o = sibling_slot(v, row0, frames, f, g2, j);
-      if (o < 0) continue;
-      const double other = cand[o];
-      if (!(other > 0.0) || !same_key(key, keys[o])) continue;
+    for (unsigned m = siblings; m; m &= m - 1) {
+      const int g2 = __ffs(m) - 1;
+      const double other = cand[sibling_slot(v, row0, frames, f, g2, j)];
       fix_f0_score(inst, harmonics, value, other, v.f0_floor, v.f0_ceil, f0, score);
       refined[gf * v.capacity + g2 * K + j] = f0;
       scores[gf * v.capacity + g2 * K + j] = score;
