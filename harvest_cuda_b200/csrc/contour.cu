@@ -28,25 +28,35 @@ __host__ __device__ inline int64_t contour_scratch_doubles(int64_t frames) {
 
 // GetBoundaryList (harvest.cpp:727-743) over f(0..len), by all 32 lanes:
 // voicing changes are found 32 frames at a time with a ballot, and change
-// number idx is stored as i - idx % 2. Returns the count on every lane.
+// number idx is stored as i - idx % 2. Four groups of 32 frames are loaded
+// before their ballots are taken in order. Returns the count on every lane.
 template <class F>
 __device__ int warp_boundary_list(F f, int len, int* out) {
+  constexpr int kGroups = 4;
   const int lane = threadIdx.x & 31;
   int count = 0;
-  for (int base = 1; base < len; base += 32) {
-    const int i = base + lane;
-    bool change = false;
-    if (i < len) {
-      int now = (i == len - 1) ? 0 : (f(i) > 0 ? 1 : 0);
-      int before = (i - 1 == 0) ? 0 : (f(i - 1) > 0 ? 1 : 0);
-      change = now != before;
+  for (int base = 1; base < len; base += 32 * kGroups) {
+    bool change[kGroups];
+#pragma unroll
+    for (int u = 0; u < kGroups; ++u) {
+      const int i = base + 32 * u + lane;
+      change[u] = false;
+      if (i < len) {
+        int now = (i == len - 1) ? 0 : (f(i) > 0 ? 1 : 0);
+        int before = (i - 1 == 0) ? 0 : (f(i - 1) > 0 ? 1 : 0);
+        change[u] = now != before;
+      }
     }
-    const unsigned mask = __ballot_sync(kAll, change);
-    if (change) {
-      int idx = count + __popc(mask & ((1u << lane) - 1));
-      out[idx] = i - idx % 2;
+#pragma unroll
+    for (int u = 0; u < kGroups; ++u) {
+      const int i = base + 32 * u + lane;
+      const unsigned mask = __ballot_sync(kAll, change[u]);
+      if (change[u]) {
+        int idx = count + __popc(mask & ((1u << lane) - 1));
+        out[idx] = i - idx % 2;
+      }
+      count += __popc(mask);
     }
-    count += __popc(mask);
   }
   __syncwarp();
   return count;
@@ -373,16 +383,29 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
   double* shared_tail = tails + 32 * kTransient;                     // F + 600
   int* deferred = reinterpret_cast<int*>(shared_tail + F + 600);     // (F + 602) ints
 
-  // FixStep1 (harvest.cpp:710-722), allowed range 0.008.
-  for (int i = lane; i < F; i += 32) {
-    double out = 0.0;
-    if (i >= 2 && base[i] != 0.0) {
-      double ref = base[i - 1] * 2 - base[i - 2];
-      out = fabs((base[i] - ref) / ref) > 0.008 &&
-            fabs((base[i] - base[i - 1])) / base[i - 1] > 0.008 ? 0.0 : base[i];
+  // FixStep1 (harvest.cpp:710-722), allowed range 0.008; four groups of 32
+  // frames per iteration.
+  for (int i0 = lane; i0 < F; i0 += 128) {
+    double b0[4], b1[4], b2[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + 32 * u;
+      b0[u] = i < F ? base[i] : 0.0;
+      b1[u] = i < F && i >= 2 ? base[i - 1] : 0.0;
+      b2[u] = i < F && i >= 2 ? base[i - 2] : 0.0;
     }
-    s1[i] = out;
-    s2[i] = out;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = i0 + 32 * u;
+      if (i >= F) break;
+      double out = 0.0;
+      if (i >= 2 && b0[u] != 0.0) {
+        double ref = b1[u] * 2 - b2[u];
+        out = fabs((b0[u] - ref) / ref) > 0.008 && fabs((b0[u] - b1[u])) / b1[u] > 0.008 ? 0.0 : b0[u];
+      }
+      s1[i] = out;
+      s2[i] = out;
+    }
   }
   __syncwarp();
   // FixStep2 (harvest.cpp:748-762): voiced runs shorter than 7 frames go.
