@@ -34,8 +34,9 @@ __global__ void make_twiddles(double2* __restrict__ tw) {
 }
 
 // Forward real FFT of the 8192 samples in `buf` (packed as z[m] = x[2m] +
-// i x[2m+1]) into spectrum[0..4096].
-__device__ void real_forward(double2* buf, const double2* __restrict__ tw, double2* __restrict__ out) {
+// i x[2m+1]): emit(k, X[k]) for k = 0..4096.
+template <class Emit>
+__device__ void real_forward(double2* buf, const double2* __restrict__ tw, Emit emit) {
   __syncthreads();
   fft4096<-1>(buf, tw);
   for (int k = threadIdx.x; k <= kHalfN; k += kFftThreads) {
@@ -44,12 +45,14 @@ __device__ void real_forward(double2* buf, const double2* __restrict__ tw, doubl
     const double2 e = make_double2(0.5 * (a.x + b.x), 0.5 * (a.y + b.y));
     const double2 d = csub(a, b);
     const double2 o = make_double2(0.5 * d.y, -0.5 * d.x);  // d / (2i)
-    out[k] = cadd(e, cmul(twiddle<-1>(tw, k), o));
+    emit(k, cadd(e, cmul(twiddle<-1>(tw, k), o)));
   }
 }
 
 // One spectrum per block of every clip; block j of clip c holds
-// y[j V - H + 1 + p], p < 8192 (zero outside the clip).
+// y[j V - H + 1 + p], p < 8192 (zero outside the clip). Each bin is turned by
+// e^{-2 pi i k H / 8192}, the linear phase of every band's filter (below),
+// so that the bands' products need only real amplitudes.
 __global__ void __launch_bounds__(kFftThreads)
 block_spectra(BatchView v, FftBankGeometry g, const double* __restrict__ y,
               const double2* __restrict__ tw, double2* __restrict__ spectra) {
@@ -65,14 +68,20 @@ block_spectra(BatchView v, FftBankGeometry g, const double* __restrict__ y,
     buf[fpad(m)] = make_double2(p0 >= 0 && p0 < y_len ? y[y0 + p0] : 0.0,
                                 p1 >= 0 && p1 < y_len ? y[y0 + p1] : 0.0);
   }
-  real_forward(buf, tw, spectra + static_cast<int64_t>(blk) * (kHalfN + 1));
+  double2* out = spectra + static_cast<int64_t>(blk) * (kHalfN + 1);
+  const int H = g.max_half;
+  real_forward(buf, tw, [&](int k, double2 x) { out[k] = cmul(x, twiddle<-1>(tw, k * H)); });
 }
 
 // Per band the spectrum of g_b[p] = h_b[p - (H - h_b)], p in [H - h_b, H + h_b].
+// g_b is symmetric about p = H (h_b is a window times a cosine centred on its
+// middle tap), so G_b[k] = A_b[k] e^{-2 pi i k H / 8192} with A_b real; the
+// amplitudes A_b[k] (the real part after removing the phase; the imaginary
+// part is rounding) are stored.
 __global__ void __launch_bounds__(kFftThreads)
 filter_spectra(const int* __restrict__ half, const int64_t* __restrict__ tap_off,
                const double* __restrict__ taps_rev, int max_half, const double2* __restrict__ tw,
-               double2* __restrict__ filters) {
+               double* __restrict__ amps) {
   extern __shared__ double2 buf[];
   const int b = blockIdx.x;
   const int h = half[b];
@@ -82,12 +91,13 @@ filter_spectra(const int* __restrict__ half, const int64_t* __restrict__ tap_off
     return m >= 0 && m <= 2 * h ? taps[2 * h - m] : 0.0;
   };
   for (int m = threadIdx.x; m < kHalfN; m += kFftThreads) buf[fpad(m)] = make_double2(tap(2 * m), tap(2 * m + 1));
-  real_forward(buf, tw, filters + static_cast<int64_t>(b) * (kHalfN + 1));
+  double* out = amps + static_cast<int64_t>(b) * (kHalfN + 1);
+  real_forward(buf, tw, [&](int k, double2 x) { out[k] = cmul(x, twiddle<+1>(tw, k * max_half)).x; });
 }
 
 __global__ void __launch_bounds__(kFftThreads, 2)
 band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra,
-              const double2* __restrict__ filters, const double2* __restrict__ tw,
+              const double* __restrict__ amps, const double2* __restrict__ tw,
               const double* __restrict__ edge_bins, int* __restrict__ queue, double* __restrict__ slots,
               double* __restrict__ raw) {
   extern __shared__ double2 buf[];
@@ -116,7 +126,7 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
     double c0, c1r, c1i;
     final_bin_terms(v.taps_rev + v.tap_off[b], half, n, edge_bins + 3 * c,
                     static_cast<double>(kRealN) / n, red, c0, c1r, c1i);
-    const double2* G = filters + static_cast<int64_t>(b) * (kHalfN + 1);
+    const double* A = amps + static_cast<int64_t>(b) * (kHalfN + 1);
     const int64_t blk0 = g.blk_off[c], blocks = g.blk_off[c + 1] - blk0;
     FinalBinTerm fb;
     fb.c0 = c0;
@@ -132,8 +142,10 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
       // Spectrum product and packing for the inverse real transform:
       // Z[k] = (X[k] + conj X[M-k]) + i e^{+2 pi i k / 8192} (X[k] - conj X[M-k]).
       for (int k = tid; k <= kHalfN / 2; k += kFftThreads) {
-        const double2 xk = cmul(Y[k], G[k]);
-        const double2 xm = cmul(Y[kHalfN - k], G[kHalfN - k]);
+        const double2 yk = Y[k], ym = Y[kHalfN - k];
+        const double ak = A[k], am = A[kHalfN - k];
+        const double2 xk = make_double2(yk.x * ak, yk.y * ak);
+        const double2 xm = make_double2(ym.x * am, ym.y * am);
         const double2 w = twiddle<+1>(tw, k);
         buf[fpad(k)] = cadd(cadd(xk, conj2(xm)), rot90<+1>(cmul(w, csub(xk, conj2(xm)))));
         if (k != 0 && k != kHalfN / 2) {
@@ -253,18 +265,18 @@ cudaError_t launch_twiddles(double2* tw, cudaStream_t stream) {
 }
 
 cudaError_t launch_filter_spectra(const int* half, const int64_t* tap_off, const double* taps_rev, int bands,
-                                  int max_half, const double2* tw, double2* filters, cudaStream_t stream) {
+                                  int max_half, const double2* tw, double* amps, cudaStream_t stream) {
   filter_spectra<<<bands, kFftThreads, fft_bank_smem_bytes(), stream>>>(half, tap_off, taps_rev, max_half, tw,
-                                                                         filters);
+                                                                         amps);
   return cudaGetLastError();
 }
 
 cudaError_t launch_fft_bank(const BankView& v, const FftBankGeometry& g, const double* y, const double* edge_bins,
-                            const double2* tw, const double2* filters, double2* spectra, int* queue,
+                            const double2* tw, const double* amps, double2* spectra, int* queue,
                             double* slots, int ctas, double* raw, cudaStream_t stream) {
   block_spectra<<<static_cast<unsigned>(g.total_blocks), kFftThreads, fft_bank_smem_bytes(), stream>>>(
       v.batch, g, y, tw, spectra);
-  band_bank_fft<<<ctas, kFftThreads, fft_bank_smem_bytes(), stream>>>(v, g, spectra, filters, tw, edge_bins,
+  band_bank_fft<<<ctas, kFftThreads, fft_bank_smem_bytes(), stream>>>(v, g, spectra, amps, tw, edge_bins,
                                                                       queue, slots, raw);
   return cudaGetLastError();
 }

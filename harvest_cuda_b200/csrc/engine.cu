@@ -316,7 +316,7 @@ struct Plan {
   double *d_centre, *d_taps;
   int2* d_items;
   int64_t* d_blk_off = nullptr;
-  double2* filters = nullptr;  // [bands][4097] filter spectra of the FFT bank
+  double* filters = nullptr;   // [bands][4097] filter amplitudes of the FFT bank
   // Refinement launch shape, chosen by the autotuner on the plan's first run.
   RefineShape refine_shape;
   bool tuned = false;
@@ -333,7 +333,7 @@ struct Plan {
 // settings, so that planning a new batch shape allocates nothing on the device.
 struct DeviceBank {
   void* tables = nullptr;
-  double2* filters = nullptr;       // [bands][block / 2 + 1]
+  double* filters = nullptr;        // [bands][block / 2 + 1] real amplitudes
   double* centre = nullptr;
   int* half = nullptr;
   int64_t* tap_off = nullptr;
@@ -470,7 +470,7 @@ struct Workspace {
     if (spectra && !b.filters) {
       if (fft_bank_ctas_per_sm() < 1) throw RuntimeFailure("FFT band-bank kernel does not fit on this device");
       const int block = fft_bank_block_length();
-      check(cudaMalloc(&b.filters, sizeof(double2) * (block / 2 + 1) * bank.bands), "cudaMalloc(filters)");
+      check(cudaMalloc(&b.filters, sizeof(double) * (block / 2 + 1) * bank.bands), "cudaMalloc(filters)");
       check(launch_filter_spectra(b.half, b.tap_off, b.taps, bank.bands, bank.max_half, twiddles, b.filters,
                                   stream),
             "filter_spectra");

@@ -140,9 +140,9 @@ int fft_bank_block_length();
 int fft_bank_ctas_per_sm();
 cudaError_t launch_twiddles(double2* tw, cudaStream_t stream);
 cudaError_t launch_filter_spectra(const int* half, const int64_t* tap_off, const double* taps_rev, int bands,
-                                  int max_half, const double2* tw, double2* filters, cudaStream_t stream);
+                                  int max_half, const double2* tw, double* amps, cudaStream_t stream);
 cudaError_t launch_fft_bank(const BankView& v, const FftBankGeometry& g, const double* y, const double* edge_bins,
-                            const double2* tw, const double2* filters, double2* spectra, int* queue,
+                            const double2* tw, const double* amps, double2* spectra, int* queue,
                             double* slots, int ctas, double* raw, cudaStream_t stream);
 
 cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t total_frames,
