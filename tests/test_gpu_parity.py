@@ -75,6 +75,21 @@ def test_short_silent_input(gpu, checker, length):
     np.testing.assert_array_equal(actual[1], expected[1])
 
 
+@pytest.mark.parametrize("seconds,fs,period", [(4.0, 16000, 5.0), (9.0, 44100, 1.0)])
+def test_long_voiced_section(gpu, checker, seconds, fs, period):
+    # One voiced section longer than 2048 frames: the engine smooths it with
+    # the whole warp in warmed-up chunks instead of one sequential pass; its
+    # F0 must stay within rounding of the sequential result.
+    x = signals.glide_clip(seconds, fs, edge=0.2, seed=12)[0]
+    expected = checker.harvest(x, fs, 71.0, 800.0, period)
+    actual = hv.harvest(x, fs, 71.0, 800.0, period)
+    assert np.count_nonzero(expected[0]) * period > 2100
+    np.testing.assert_array_equal(actual[1], expected[1])
+    both = (actual[0] > 0) & (expected[0] > 0)
+    assert np.array_equal(actual[0] > 0, expected[0] > 0)
+    assert np.max(np.abs(actual[0][both] - expected[0][both]) / expected[0][both]) <= 1e-10
+
+
 def test_separate_voiced_sections(gpu, checker):
     fs = 16000
     t = np.arange(fs * 8) / fs
