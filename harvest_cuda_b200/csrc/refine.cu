@@ -230,18 +230,20 @@ __device__ __forceinline__ void walk_window(const CandidateWindow& cw, double fs
   };
   double nc, ns;
   phase(0, nc, ns);
+  // The Blackman window as candidate_spectra forms it.
+  auto blackman = [](double c) { return fma(fma(0.16, c, 0.5), c, 0.34); };
   double w_prev = 0.0;
-  double w_cur = 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0);
+  double w_cur = blackman(nc);
   for (int i0 = 0; i0 < len; i0 += kAnchor) {
 #pragma unroll
     for (int h = 0; h < 6; ++h) {
-      long long m = (static_cast<long long>(cw.bin[h]) * i0) % n;
+      long long m = (static_cast<long long>(cw.bin[h]) * i0) & (n - 1);
       sincospi(-2.0 * static_cast<double>(m) / n, &ti[h], &tr[h]);
     }
     phase(i0 + 1, nc, ns);
     const int i1 = imin(i0 + kAnchor, len);
     for (int i = i0; i < i1; ++i) {
-      const double w_next = (i + 1 < len) ? 0.42 + 0.5 * nc + 0.08 * (2.0 * nc * nc - 1.0) : 0.0;
+      const double w_next = (i + 1 < len) ? blackman(nc) : 0.0;
       const double dw = -(w_next - w_prev) / 2.0;
       body(i, w_cur, dw, tr, ti);
 #pragma unroll
