@@ -367,7 +367,9 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
 __device__ __forceinline__ double fix_f0_frequencies(const HarmonicSpectra& sp, const CandidateWindow& cw,
                                                      double fs, double inst[6]) {
   double num = 0.0, den = 0.0;
-#pragma unroll
+  // Rolled: the per-job code stays small (instruction fetch limits the
+  // refinement more than these few iterations do).
+#pragma unroll 1
   for (int h = 0; h < 6; ++h) {
     inst[h] = 0.0;
     if (h >= cw.harmonics) continue;
@@ -384,9 +386,8 @@ __device__ __forceinline__ double fix_f0_frequencies(const HarmonicSpectra& sp, 
 __device__ __forceinline__ void fix_f0_score(const double inst[6], int harmonics, double refined, double f0c,
                                              double f0_floor, double f0_ceil, double& out_f0, double& out_score) {
   double err = 0.0;
-#pragma unroll
-  for (int h = 0; h < 6; ++h)
-    if (h < harmonics) err += fabs((inst[h] / (h + 1.0) - f0c) / f0c);
+#pragma unroll 1
+  for (int h = 0; h < harmonics; ++h) err += fabs((inst[h] / (h + 1.0) - f0c) / f0c);
   double score = 1.0 / (err / harmonics + kGuard);
   if (refined < f0_floor || refined > f0_ceil || score < 2.5) refined = score = 0.0;
   out_f0 = refined;
