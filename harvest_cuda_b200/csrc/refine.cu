@@ -395,16 +395,16 @@ __device__ __forceinline__ void fix_f0_score(const double inst[6], int harmonics
 }
 
 // One thread per job, grid-stride over the job list (longest windows first).
-// A job's spectra also serve every later overlap sibling (same candidate,
-// group g2 > g) with the same window and bins: those cells get FixF0 with
-// their own initial F0, which changes only the score. kMinBlocks caps registers so that that many 128-thread blocks fit on an
-// SM; the autotuner picks the instance and the grid (RefineShape).
+// A job's spectra also serve the later overlap siblings (same candidate,
+// group g2 > g) with the same window and bins, named by the job key's sibling
+// bits: those cells get FixF0 with their own initial F0, which changes only
+// the score. kMinBlocks caps registers so that that many 128-thread blocks
+// fit on an SM; the autotuner picks the instance and the grid (RefineShape).
 template <int kMinBlocks>
 __global__ void __launch_bounds__(128, kMinBlocks)
 refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restrict__ jobs,
             const int* __restrict__ total, const double* __restrict__ cand, const int* __restrict__ count,
-            const ulonglong2* __restrict__ keys, const double2* __restrict__ tw, double* __restrict__ refined,
-            double* __restrict__ scores) {
+            const double2* __restrict__ tw, double* __restrict__ refined, double* __restrict__ scores) {
   const int total_jobs = *total;
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total_jobs; idx += gridDim.x * blockDim.x) {
     const RefineJob job = jobs[idx];
@@ -524,7 +524,7 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
                                                 b.class_cursor, b.jobs, refined, scores);
   const unsigned job_grid = static_cast<unsigned>(sms * shape.blocks_per_sm);
   auto kernel = shape.min_blocks == 4 ? refine_jobs<4> : (shape.min_blocks == 5 ? refine_jobs<5> : refine_jobs<1>);
-  kernel<<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, cand, count, b.keys, b.twiddles, refined, scores);
+  kernel<<<job_grid, 128, 0, stream>>>(v, y, b.jobs, b.total, cand, count, b.twiddles, refined, scores);
   return cudaGetLastError();
 }
 
