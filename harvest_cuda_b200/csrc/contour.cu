@@ -299,15 +299,29 @@ __device__ void smooth_section_warp(P padded, int st, int ed, int64_t len, doubl
   const double head = padded(st), tail_value = padded(ed);
   const int n = ed - st + 1, chunk = (n + 31) / 32;
   const int c0 = imin(st + lane * chunk, ed + 1), c1 = imin(c0 + chunk, ed + 1);   // this lane's [c0, c1)
+  constexpr int kAhead = 2 * kChunk;   // inputs loaded ahead into registers
   // Forward body.
   Butter fw;
+  auto forward = [&](int from, int to, bool store) {   // steps from .. to - 1
+    for (int j0 = from; j0 < to; j0 += kAhead) {
+      double in[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) in[k] = j0 + k < to ? padded(j0 + k) : 0.0;
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) {
+        if (j0 + k >= to) break;
+        const double o = fw.step(in[k]);
+        if (store) out[j0 + k - lag] = o;
+      }
+    }
+  };
   int j = c0 - kWarm;
   if (j <= st) {
     fw.run_constant(head, st);
     j = st;
   }
-  for (; j < c0; ++j) fw.step(padded(j));
-  for (; j < c1; ++j) out[j - lag] = fw.step(padded(j));
+  forward(j, c0, false);
+  forward(c0, c1, true);
   __syncwarp();                        // forward outputs visible to every lane
   const int owner = (n - 1) / chunk;   // lane whose chunk ends at ed
   fw.w0 = __shfl_sync(kAll, fw.w0, owner);
@@ -339,22 +353,42 @@ __device__ void smooth_section_warp(P padded, int st, int ed, int64_t len, doubl
       re.w0 = saved[2 * (first / stretch)];
       re.w1 = saved[2 * (first / stretch) + 1];
       for (int64_t k = 0; k < m; ++k) tail[k] = re.step(tail_value);
-      for (int64_t k = m - 1; k >= 0; --k) bw.step(tail[k]);
+      for (int64_t k0 = m - 1; k0 >= 0; k0 -= kAhead) {
+        double in[kAhead];
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) in[k] = k0 - k >= 0 ? tail[k0 - k] : 0.0;
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k)
+          if (k0 - k >= 0) bw.step(in[k]);
+      }
     }
   }
   const double t0 = __shfl_sync(kAll, bw.w0, 0), t1 = __shfl_sync(kAll, bw.w1, 0);
   // Backward body: every lane first runs its warm-up over forward outputs of
   // later chunks, then (after all have) overwrites its own chunk.
   Butter b;
+  auto backward = [&](int from, int to, bool store) {   // steps from down to to
+    for (int j0 = from; j0 >= to; j0 -= kAhead) {
+      double in[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) in[k] = j0 - k >= to ? out[j0 - k - lag] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) {
+        if (j0 - k < to) break;
+        const double o = b.step(in[k]);
+        if (store) out[j0 - k - lag] = o;
+      }
+    }
+  };
   j = c1 - 1 + kWarm;
   if (j >= ed) {
     b.w0 = t0;
     b.w1 = t1;
     j = ed;
   }
-  for (; j >= c1; --j) b.step(out[j - lag]);
+  backward(j, c1, false);
   __syncwarp();
-  for (; j >= c0; --j) out[j - lag] = b.step(out[j - lag]);
+  backward(c1 - 1, c0, true);
   __syncwarp();
 }
 
