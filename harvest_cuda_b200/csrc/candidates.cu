@@ -9,8 +9,8 @@ namespace hv {
 // thread per frame walks the bands: runs of at least 10 voiced channels
 // (first and last channel forced unvoiced) become one candidate, their mean
 // summed in channel order. `cand` is [frame][per_group]; per-clip maxima go
-// to count[] (zeroed by the caller). Bands are loaded 8 at a time (the loads
-// of a group are independent), and each run's sum is carried along the walk:
+// to count[] (zeroed by the caller), one atomic per clip per warp. Bands are
+// loaded 16 at a time (the loads of a group are independent), and each run's sum is carried along the walk:
 // the same additions, from 0, in channel order, as the reference's loop.
 __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
                                     int64_t total_frames, double* __restrict__ cand,
@@ -20,15 +20,15 @@ __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
   double* row = cand + gf * v.per_group;
   int found = 0, start = 0, prev = 0;
   double run = 0.0;
-  for (int b0 = 1; b0 < v.bands; b0 += 8) {
-    double r[8];
+  for (int b0 = 1; b0 < v.bands; b0 += 16) {
+    double r[16];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < 16; ++u) {
       const int b = b0 + u;
       r[u] = b < v.bands - 1 ? raw[b * total_frames + gf] : 0.0;
     }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < 16; ++u) {
       const int b = b0 + u;
       if (b >= v.bands) break;
       const int now = (b == v.bands - 1) ? 0 : (r[u] > 0 ? 1 : 0);
@@ -47,7 +47,12 @@ __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
   for (int j = found; j < v.per_group; ++j) row[j] = 0.0;
   // At most (bands - 1) / 11 runs fit, fewer than per_group; the clamp only
   // keeps later column arithmetic in bounds.
-  if (found) atomicMax(count + owner(v.frame_off, v.clips, gf), imin(found, v.per_group));
+  // Lanes of the same clip take their maximum first (the counters only
+  // grow, so the order of the atomics does not matter).
+  const int c = owner(v.frame_off, v.clips, gf);
+  const unsigned peers = __match_any_sync(__activemask(), c);
+  const int m = __reduce_max_sync(peers, static_cast<unsigned>(imin(found, v.per_group)));
+  if (m > 0 && (threadIdx.x & 31) == __ffs(peers) - 1) atomicMax(count + c, m);
 }
 
 // a13: RemoveUnreliableCandidates(Sub) with SelectBestF0 (harvest.cpp:636-688)
