@@ -153,24 +153,70 @@ CLOCK_QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.ac
 
 
 class ClockSampler:
-    """Samples nvidia-smi every 200 ms while the timed region runs."""
+    """Samples the SM clock and the clock-event reasons while the timed
+    region runs: through NVML every 10 ms (read-only queries, in a thread;
+    the first sample is taken before the region starts), else nvidia-smi
+    every 200 ms."""
+
+    REASONS = (("hw_slowdown", "HwSlowdown"), ("hw_thermal_slowdown", "HwThermalSlowdown"),
+               ("sw_thermal_slowdown", "SwThermalSlowdown"), ("sw_power_cap", "SwPowerCap"))
 
     def __init__(self, device):
         self.device = device
         self.proc = None
+        self.thread = None
+        self.samples = []       # (sm MHz, max sm MHz, set of reasons)
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.device)
+        bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+        return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+
+    def _nvml_sample(self, nv, h, mx):
+        mask = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        reasons = {name for name, suffix in self.REASONS
+                   if mask & getattr(nv, "nvmlClocksEventReason" + suffix)}
+        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), mx, reasons))
 
     def __enter__(self):
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._nvml_sample(nv, h, mx)
+        except Exception:           # no NVML binding or device: fall back to nvidia-smi
+            nv = None
+        if nv is not None:
+            self.source = "nvml, 10 ms"
+            self._stop = threading.Event()
+
+            def loop():
+                while not self._stop.wait(0.01):
+                    try:
+                        self._nvml_sample(nv, h, mx)
+                    except Exception:
+                        return
+            self.thread = threading.Thread(target=loop, daemon=True)
+            self.thread.start()
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device), f"--query-gpu={CLOCK_QUERY}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.source = "nvidia-smi, 200 ms"
         except OSError:
             self.proc = None
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        if self.thread is not None:
+            self._stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -178,27 +224,25 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+            for ln in out.splitlines():
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm, mx = float(parts[1]), float(parts[2])
+                except ValueError:
+                    continue
+                reasons = {name for (name, _), flag in zip(self.REASONS, parts[5:9])
+                           if flag.lower() == "active"}
+                self.samples.append((sm, mx, reasons))
 
     def summary(self):
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        sm, mx, reasons = [], None, set()
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                mx = float(parts[2])
-            except ValueError:
-                continue
-            for name, flag in zip(names, parts[5:9]):
-                if flag.lower() == "active":
-                    reasons.add(name)
-        if not sm:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        reasons = set().union(*(r for _, _, r in self.samples))
+        return {"sm_mhz": statistics.median(sm for sm, _, _ in self.samples),
+                "sm_max_mhz": self.samples[-1][1], "reasons": sorted(reasons),
+                "samples": len(self.samples), "source": self.source}
 
 
 # ------------------------------------------------------- CPU baseline --
