@@ -127,7 +127,7 @@ raw_adjoint(RawAdjointView v) {
       const double* gr = v.grad_raw + static_cast<int64_t>(b) * v.total_frames + f_begin;
       int seg[4], last[4], lo[4], hi[4];
       double x0[4], x1[4], y0v[4], y1v[4], ez[4], ea[4], eb[4];
-      const double t0 = fa * 1 / 1000.0;
+      const double t0 = frame_seconds(fa);
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         last[k] = count[k] - 2;
@@ -157,7 +157,7 @@ raw_adjoint(RawAdjointView v) {
         y1v[k] = fs / (eb[k] - ea[k]);
       }
       for (int f = fa; f < fb; ++f) {
-        const double t = f * 1 / 1000.0;
+        const double t = frame_seconds(f);
         for (;;) {
           bool any = false;
 #pragma unroll

@@ -48,4 +48,16 @@ __device__ __forceinline__ int owner(const int64_t* off, int clips, int64_t row)
 __device__ __forceinline__ int imin(int a, int b) { return a < b ? a : b; }
 __device__ __forceinline__ int imax(int a, int b) { return a > b ? a : b; }
 
+// Time of 1 ms frame f in seconds: f / 1000.0 correctly rounded (WORLD's
+// `i * 1 / 1000.0`), without a division. q = RN(f * RN(1/1000)) is
+// corrected once by its exact remainder RN(f - 1000 q) (Markstein's scheme
+// for a constant divisor); the result equals the IEEE quotient for every
+// int f >= 0.
+__device__ __forceinline__ double frame_seconds(int f) {
+  constexpr double kInv = 1.0 / 1000.0;
+  const double x = static_cast<double>(f);
+  const double q = __dmul_rn(x, kInv);
+  return __fma_rn(__fma_rn(-q, 1000.0, x), kInv, q);
+}
+
 }  // namespace hv

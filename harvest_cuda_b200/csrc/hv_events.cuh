@@ -124,7 +124,7 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
   int seg[4], last[4];
   double x0[4], x1[4], y0[4], y1[4], ea[4], eb[4];   // ea, eb: edges seg, seg + 1
   double inv[4];                                      // 1 / (x1 - x0)
-  const double t0 = fa * 1 / 1000.0;
+  const double t0 = frame_seconds(fa);
   // The first frame's segment of the four tracks, by binary searches
   // interleaved so that their dependent loads overlap.
   int lo[4], hi[4];
@@ -162,7 +162,7 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
 #pragma unroll
   for (int k = 0; k < 4; ++k) nxt[k] = ev[k][imin(seg[k] + 2, count[k] - 1)];
   for (int f = fa; f < fb; ++f) {
-    const double t = f * 1 / 1000.0;
+    const double t = frame_seconds(f);
     for (;;) {
       bool step[4], any = false;
 #pragma unroll

@@ -416,7 +416,7 @@ refine_jobs(BatchView v, const double* __restrict__ y, const RefineJob* __restri
     const int64_t row0 = v.frame_off[c];
     const int f = static_cast<int>(gf - row0);
     const int64_t y0 = v.y_off[c];
-    const double t = f * 1 / 1000.0;
+    const double t = frame_seconds(f);
     const CandidateWindow cw(v.fs_r, t, job.f0c);
     HarmonicSpectra sp;
     candidate_spectra(y + y0, static_cast<int>(v.y_off[c + 1] - y0), v.fs_r, t, cw, tw, sp);
@@ -462,7 +462,7 @@ refine_adjoint(BatchView v, const double* __restrict__ y, const double* __restri
     const int f = static_cast<int>(gf - v.frame_off[c]);
     const int64_t y0 = v.y_off[c];
     const int y_len = static_cast<int>(v.y_off[c + 1] - y0);
-    const double fs = v.fs_r, t = f * 1 / 1000.0;
+    const double fs = v.fs_r, t = frame_seconds(f);
     const CandidateWindow cw(fs, t, f0c);
     HarmonicSpectra sp;
     candidate_spectra(y + y0, y_len, fs, t, cw, tw, sp);
