@@ -193,28 +193,130 @@ struct Butter {
     w0 = wt;
     return out;
   }
-  // `steps` steps on a constant input. Once a step leaves the state
-  // unchanged every later step repeats it, so the rest is skipped; the
-  // result equals running all steps.
-  __device__ void run_constant(double x, int64_t steps) {
-    for (int64_t k = 0; k < steps; ++k) {
-      double p0 = w0, p1 = w1;
-      step(x);
-      if (w0 == p0 && w1 == p1) break;
+  // `steps` steps on a constant input. The state (w0, w1) then evolves by a
+  // fixed map, so once it equals an earlier state it repeats with that
+  // period, and the whole periods left are skipped: the result equals
+  // running all steps. A state settles within a few hundred steps into a
+  // fixed point or a rounding limit cycle (periods 4 and 8, rarely a few
+  // dozen). Each state is compared with the previous one and with a
+  // reference re-taken after 1, 2, 4, ..., 64 steps and then every 64 steps,
+  // which finds every period up to 64.
+  __device__ __forceinline__ void run_constant(double x, int64_t steps) {
+    run_rounds([x](int) { return x; }, 1, steps);
+  }
+
+  // `steps` steps on the inputs pat[0], ..., pat[p - 1], pat[0], ... The
+  // state after each round of p steps evolves by a fixed map; repeats of it
+  // are skipped as in run_constant.
+  __device__ __forceinline__ void run_periodic(const double* pat, int p, int64_t steps) {
+    run_rounds([pat](int i) { return pat[i]; }, p, steps);
+  }
+
+  template <class In>
+  __device__ __forceinline__ void run_rounds(In in, int p, int64_t steps) {
+    const int64_t rounds = steps / p;
+    double s0 = w0, s1 = w1;
+    int since = 0, every = 1;
+    for (int64_t r = 0; r < rounds; ++r) {
+      const double p0 = w0, p1 = w1;
+      for (int i = 0; i < p; ++i) step(in(i));
+      ++since;
+      int period = 0;
+      if (w0 == p0 && w1 == p1) period = 1;
+      else if (w0 == s0 && w1 == s1) period = since;
+      if (period) {
+        for (int64_t q = (rounds - r - 1) % period; q > 0; --q)
+          for (int i = 0; i < p; ++i) step(in(i));
+        break;
+      }
+      if (since == every) {
+        s0 = w0;
+        s1 = w1;
+        since = 0;
+        every = every < 64 ? 2 * every : 64;
+      }
     }
+    for (int64_t i = 0; i < steps % p; ++i) step(in(static_cast<int>(i)));
   }
 };
+
+// The held tail of a section: the forward filter `fw` runs `trailing` steps
+// on tail_value, then the backward filter `bw` runs over those outputs in
+// reverse. The forward state settles into a fixed point or a limit cycle of
+// period <= 64 (see run_constant); from there its outputs repeat with that
+// period, kept in the first 64 doubles of `tail`, and the backward pass over
+// them runs as run_periodic. The outputs before that are recomputed stretch
+// by stretch, newest first, from states checkpointed every `cap` / 2 steps
+// in the second half of `tail`, into its first half; recomputation from a
+// saved state repeats the same steps. So `bw` ends as if every output had
+// been stored. Returns false if more than cap / 4 checkpoints are needed.
+__device__ __noinline__ bool held_tail(Butter fw, double tail_value, int64_t trailing, double* tail,
+                                       int64_t cap, Butter& bw) {
+  constexpr int kAhead = 2 * kChunk;
+  constexpr int kRing = 64;
+  const int64_t stretch = cap / 2;
+  double* saved = tail + stretch;   // (w0, w1) before steps 0, stretch, 2 stretch, ...
+  double* ring = tail;              // output k at ring[k % kRing]
+  double* rpat = tail + kRing;      // the periodic outputs in reverse order
+  int64_t stored = trailing;        // outputs before the periodic part
+  int period = 0;
+  double s0 = fw.w0, s1 = fw.w1;
+  int since = 0, every = 1;
+  for (int64_t k = 0; k < trailing; ++k) {
+    if (k % stretch == 0) {
+      const int64_t c = k / stretch;
+      if (2 * c + 1 >= stretch) return false;
+      saved[2 * c] = fw.w0;
+      saved[2 * c + 1] = fw.w1;
+    }
+    const double p0 = fw.w0, p1 = fw.w1;
+    ring[k % kRing] = fw.step(tail_value);
+    ++since;
+    if (fw.w0 == p0 && fw.w1 == p1) period = 1;
+    else if (fw.w0 == s0 && fw.w1 == s1) period = since;
+    if (period) {
+      // Outputs stored .. k are one period; every later output repeats them.
+      stored = k + 1 - period;
+      break;
+    }
+    if (since == every) {
+      s0 = fw.w0;
+      s1 = fw.w1;
+      since = 0;
+      every = every < 64 ? 2 * every : 64;
+    }
+  }
+  if (period) {
+    for (int i = 0; i < period; ++i) {
+      const int64_t rel = (trailing - 1 - stored - i) % period;   // output trailing - 1 - i
+      rpat[i] = ring[(stored + rel) % kRing];
+    }
+    bw.run_periodic(rpat, period, trailing - stored);
+  }
+  for (int64_t first = (stored > 0 ? (stored - 1) / stretch : -1) * stretch; first >= 0; first -= stretch) {
+    const int64_t n = stored - first < stretch ? stored - first : stretch;
+    Butter re;
+    re.w0 = saved[2 * (first / stretch)];
+    re.w1 = saved[2 * (first / stretch) + 1];
+    for (int64_t k = 0; k < n; ++k) tail[k] = re.step(tail_value);
+    for (int64_t k0 = n - 1; k0 >= 0; k0 -= kAhead) {
+      double in[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) in[k] = k0 - k >= 0 ? tail[k0 - k] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k)
+        if (k0 - k >= 0) bw.step(in[k]);
+    }
+  }
+  return true;
+}
 
 // Smooths the voiced section [st, ed] of the padded contour (lag 300) as
 // FilteringF0 does over the whole padded length: the held head, the body
 // and the held tail forward, then everything backward. Body outputs go to
-// out[j - lag]. The forward tail runs until its state stops changing (or to
-// the end); the backward pass needs its outputs in reverse, so the forward
-// pass keeps the filter state every `cap` / 2 steps in the second half of
-// `tail` and the backward pass recomputes each stretch from its checkpoint
-// into the first half, newest first. Recomputation from a saved state
-// repeats the same steps, so this equals storing every output. Returns false
-// if the tail needs more than cap / 4 checkpoints.
+// out[j - lag]. The held head runs as run_constant and the held tail as
+// held_tail (in `tail`, cap doubles), both equal to running every step.
+// Returns false if the tail needs more than cap / 4 checkpoints.
 template <class P>
 __device__ bool smooth_section(P padded, int st, int ed, int64_t len, double* out, double* tail,
                                int64_t cap) {
@@ -231,41 +333,8 @@ __device__ bool smooth_section(P padded, int st, int ed, int64_t len, double* ou
     for (int k = 0; k < kAhead; ++k)
       if (j0 + k <= ed) out[j0 + k - lag] = fw.step(in[k]);
   }
-  const int64_t trailing = len - 1 - ed;
-  const int64_t stretch = cap / 2;
-  double* saved = tail + stretch;          // (w0, w1) before steps 0, stretch, 2 stretch, ...
-  int64_t stored = 0;                      // tail outputs before the state settled
-  double settled = 0.0;
-  bool fixed = false;
-  for (int64_t k = 0; k < trailing; ++k) {
-    if (stored % stretch == 0) {
-      const int64_t c = stored / stretch;
-      if (2 * c + 1 >= stretch) return false;
-      saved[2 * c] = fw.w0;
-      saved[2 * c + 1] = fw.w1;
-    }
-    double p0 = fw.w0, p1 = fw.w1;
-    double o = fw.step(tail_value);
-    if (fw.w0 == p0 && fw.w1 == p1) { settled = o; fixed = true; break; }
-    ++stored;
-  }
   Butter bw;
-  if (fixed) bw.run_constant(settled, trailing - stored);
-  for (int64_t first = (stored > 0 ? (stored - 1) / stretch : -1) * stretch; first >= 0; first -= stretch) {
-    const int64_t n = stored - first < stretch ? stored - first : stretch;
-    Butter re;
-    re.w0 = saved[2 * (first / stretch)];
-    re.w1 = saved[2 * (first / stretch) + 1];
-    for (int64_t k = 0; k < n; ++k) tail[k] = re.step(tail_value);
-    for (int64_t k0 = n - 1; k0 >= 0; k0 -= kAhead) {
-      double in[kAhead];
-#pragma unroll
-      for (int k = 0; k < kAhead; ++k) in[k] = k0 - k >= 0 ? tail[k0 - k] : 0.0;
-#pragma unroll
-      for (int k = 0; k < kAhead; ++k)
-        if (k0 - k >= 0) bw.step(in[k]);
-    }
-  }
+  if (!held_tail(fw, tail_value, len - 1 - ed, tail, cap, bw)) return false;
   for (int j0 = ed; j0 >= st; j0 -= kAhead) {
     double in[kAhead];
 #pragma unroll
@@ -328,41 +397,8 @@ __device__ void smooth_section_warp(P padded, int st, int ed, int64_t len, doubl
   fw.w1 = __shfl_sync(kAll, fw.w1, owner);
   // Held tail, forward and backward, on lane 0 (as in smooth_section).
   Butter bw;
-  if (lane == 0) {
-    const int64_t trailing = len - 1 - ed;
-    const int64_t stretch = cap / 2;
-    double* saved = tail + stretch;
-    int64_t stored = 0;
-    double settled = 0.0;
-    bool fixed = false;
-    for (int64_t k = 0; k < trailing; ++k) {
-      if (stored % stretch == 0) {
-        const int64_t c = stored / stretch;
-        saved[2 * c] = fw.w0;
-        saved[2 * c + 1] = fw.w1;
-      }
-      double p0 = fw.w0, p1 = fw.w1;
-      double o = fw.step(tail_value);
-      if (fw.w0 == p0 && fw.w1 == p1) { settled = o; fixed = true; break; }
-      ++stored;
-    }
-    if (fixed) bw.run_constant(settled, trailing - stored);
-    for (int64_t first = (stored > 0 ? (stored - 1) / stretch : -1) * stretch; first >= 0; first -= stretch) {
-      const int64_t m = stored - first < stretch ? stored - first : stretch;
-      Butter re;
-      re.w0 = saved[2 * (first / stretch)];
-      re.w1 = saved[2 * (first / stretch) + 1];
-      for (int64_t k = 0; k < m; ++k) tail[k] = re.step(tail_value);
-      for (int64_t k0 = m - 1; k0 >= 0; k0 -= kAhead) {
-        double in[kAhead];
-#pragma unroll
-        for (int k = 0; k < kAhead; ++k) in[k] = k0 - k >= 0 ? tail[k0 - k] : 0.0;
-#pragma unroll
-        for (int k = 0; k < kAhead; ++k)
-          if (k0 - k >= 0) bw.step(in[k]);
-      }
-    }
-  }
+  // cap is the padded length, so the checkpoints always fit.
+  if (lane == 0) held_tail(fw, tail_value, len - 1 - ed, tail, cap, bw);
   const double t0 = __shfl_sync(kAll, bw.w0, 0), t1 = __shfl_sync(kAll, bw.w1, 0);
   // Backward body: every lane first runs its warm-up over forward outputs of
   // later chunks, then (after all have) overwrites its own chunk.
