@@ -60,9 +60,13 @@ __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
 // columns, neighbour rows are read from the unpruned arrays, and the best
 // candidate is the first column holding the highest pruned score. The warp
 // first packs the nonzero candidates of the two neighbour rows into shared
-// memory (2 capacity doubles per warp), so each column's two minima run
-// over those only: a zero candidate c gives |ref - c| / ref = 1 for
-// ref > 0, which the error's cap at 1 already covers.
+// memory, so each candidate's two minima run over those only (a zero
+// candidate c gives |ref - c| / ref = 1 for ref > 0, which the error's cap
+// at 1 already covers), and packs this row's nonzero candidates, so that a
+// lane checks one of them at a time: about half of the 7 count columns are
+// zero, and with one lane per column the warp ran the minima once per 32
+// columns with most lanes idle. 5 capacity doubles of shared memory per
+// warp.
 __global__ void __launch_bounds__(128)
 prune_frames(BatchView v, const double* __restrict__ refined, const double* __restrict__ scores,
              const int* __restrict__ count, int64_t total_frames, double* __restrict__ pruned,
@@ -79,47 +83,71 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
   const int cap = v.capacity;
   const double* row = refined + gf * cap;
   const bool interior = f >= 1 && f <= frames - 2;
-  double* s_next = s_rows + (threadIdx.x >> 5) * 2 * cap;
+  double* s_next = s_rows + (threadIdx.x >> 5) * 5 * cap;
   double* s_prev = s_next + cap;
-  int n_next = 0, n_prev = 0;
-  if (interior) {
-    const unsigned below = (1u << lane) - 1u;
-    for (int base = 0; base < columns; base += 32) {
-      const int j = base + lane;
-      const double a = j < columns ? row[cap + j] : 0.0;
-      const double b = j < columns ? row[j - cap] : 0.0;
+  double* s_ref = s_prev + cap;     // this row's candidates to check, packed
+  double* s_sc = s_ref + cap;
+  int* s_col = reinterpret_cast<int*>(s_sc + cap);
+  const unsigned below = (1u << lane) - 1u;
+  int n_next = 0, n_prev = 0, n_cur = 0;
+  double top = 0.0, pick = 0.0;
+  int top_col = cap;
+  // Highest pruned score, first column on ties.
+  auto consider = [&](double sc, double ref, int col) {
+    if (sc > top || (sc == top && col < top_col)) {
+      top = sc;
+      pick = ref;
+      top_col = col;
+    }
+  };
+  // Columns from 7 count on hold no candidate; they are neither read nor
+  // written (every reader stops at 7 count). Columns that need no check are
+  // written here; the others are packed, so that the checks below keep
+  // every lane busy.
+  for (int base = 0; base < columns; base += 32) {
+    const int j = base + lane;
+    const bool in = j < columns;
+    const double ref = in ? row[j] : 0.0, sc = in ? scores[gf * cap + j] : 0.0;
+    if (interior) {
+      const double a = in ? row[cap + j] : 0.0;
+      const double b = in ? row[j - cap] : 0.0;
       const unsigned ma = __ballot_sync(0xffffffffu, a != 0.0), mb = __ballot_sync(0xffffffffu, b != 0.0);
       if (a != 0.0) s_next[n_next + __popc(ma & below)] = a;
       if (b != 0.0) s_prev[n_prev + __popc(mb & below)] = b;
       n_next += __popc(ma);
       n_prev += __popc(mb);
     }
-    __syncwarp();
-  }
-  double top = 0.0, pick = 0.0;
-  int top_col = cap;
-  // Columns from 7 count on hold no candidate; they are neither read nor
-  // written (every reader stops at 7 count).
-  for (int col = lane; col < columns; col += 32) {
-    double ref = row[col], sc = scores[gf * cap + col];
-    if (interior && ref != 0) {
-      // SelectBestF0 leaves min(1, min_j |ref - c_j| / ref) as the error.
-      // Correctly rounded division by the same positive ref is monotone, so
-      // that equals the quotient of the smallest difference: one division
-      // per neighbour row, bit-identical. With no nonzero neighbour the
-      // quotient is infinite and the cap gives 1.
-      double d1 = __longlong_as_double(0x7ff0000000000000ll), d2 = d1;
-      for (int j = 0; j < n_next; ++j) d1 = fmin(d1, fabs(ref - s_next[j]));
-      for (int j = 0; j < n_prev; ++j) d2 = fmin(d2, fabs(ref - s_prev[j]));
-      double e1 = d1 / ref, e2 = d2 / ref;
-      if (e1 > 1.0) e1 = 1.0;
-      if (e2 > 1.0) e2 = 1.0;
-      double e = e1 < e2 ? e1 : e2;
-      if (!(e <= 0.05)) ref = sc = 0.0;
+    const bool check = in && interior && ref != 0.0;
+    const unsigned mc = __ballot_sync(0xffffffffu, check);
+    if (check) {
+      const int k = n_cur + __popc(mc & below);
+      s_ref[k] = ref;
+      s_sc[k] = sc;
+      s_col[k] = j;
+    } else if (in) {
+      pruned[gf * cap + j] = ref;
+      pruned_scores[gf * cap + j] = sc;
+      consider(sc, ref, j);
     }
+    n_cur += __popc(mc);
+  }
+  __syncwarp();
+  for (int k = lane; k < n_cur; k += 32) {
+    double ref = s_ref[k], sc = s_sc[k];
+    const int col = s_col[k];
+    // SelectBestF0 leaves min(1, min_j |ref - c_j| / ref) as the error.
+    // Correctly rounded division by the same positive ref is monotone, so
+    // the smaller of the two rows' errors is the quotient of the smaller
+    // difference: one division, bit-identical, and the cap at 1 does not
+    // change the test. With no nonzero neighbour the quotient is infinite.
+    double d1 = __longlong_as_double(0x7ff0000000000000ll), d2 = d1;
+    for (int j = 0; j < n_next; ++j) d1 = fmin(d1, fabs(ref - s_next[j]));
+    for (int j = 0; j < n_prev; ++j) d2 = fmin(d2, fabs(ref - s_prev[j]));
+    const double e = fmin(d1, d2) / ref;
+    if (!(e <= 0.05)) ref = sc = 0.0;
     pruned[gf * cap + col] = ref;
     pruned_scores[gf * cap + col] = sc;
-    if (sc > top) { top = sc; pick = ref; top_col = col; }
+    consider(sc, ref, col);
   }
   for (int o = 16; o; o >>= 1) {
     double ot = __shfl_down_sync(0xffffffffu, top, o);
@@ -141,9 +169,9 @@ cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t tot
 cudaError_t launch_prune(const BatchView& v, const double* refined, const double* scores,
                          const int* count, int64_t total_frames, double* pruned,
                          double* pruned_scores, double* best, cudaStream_t stream) {
-  // Up to 4 warps per block, each with 2 capacity doubles of shared memory,
-  // within the default 48 KB (capacity < 1024).
-  const size_t per_warp = 2 * sizeof(double) * static_cast<size_t>(v.capacity);
+  // Up to 4 warps per block, each with 5 capacity doubles of shared memory,
+  // within the default 48 KB.
+  const size_t per_warp = 5 * sizeof(double) * static_cast<size_t>(v.capacity);
   const int warps = static_cast<int>(std::max<size_t>(1, std::min<size_t>(4, 49152 / per_warp)));
   prune_frames<<<static_cast<unsigned>((total_frames + warps - 1) / warps), 32 * warps, warps * per_warp, stream>>>(
       v, refined, scores, count, total_frames, pruned, pruned_scores, best);
