@@ -177,25 +177,50 @@ band_bank_fft(BankView v, FftBankGeometry g, const double2* __restrict__ spectra
       const double* mine_lin = xs + q_lo + min(tid, edge_end / run + 1);
       auto X = [&](int i) -> double { return mine_lin[i + (i >= run ? 1 : 0)]; };
       const int len = q_hi - q_lo;   // run <= 32: hits fit one bit mask per kind
+      // The four detectors compare each sample with zero and with its
+      // neighbour: a sample is > 0 (pos) or < 0 (neg) by its sign and
+      // magnitude bits, and a difference of two samples, rounded, has the
+      // sign of their comparison. So with bit i of pos/neg for sample i and
+      // of up/down for sample i + 1 > / < sample i, a hit at i is a set bit
+      // i whose bit i + 1 is clear: pos then not pos (0 < f0, f1 <= 0), neg
+      // then not neg, up then not up (0 < f1 - f0, f2 - f1 <= 0), down then
+      // not down. Bits past sample len + 1 are never used.
       unsigned hits[4] = {0u, 0u, 0u, 0u};
-      for (int i0 = 0; i0 < len; i0 += 8) {
-        double v[10];
-#pragma unroll
-        for (int u = 0; u < 10; ++u) v[u] = X(i0 + u);
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int i = i0 + u;
-          if (i >= len) break;
-          const double f0 = v[u], f1 = v[u + 1], f2 = v[u + 2];
-          const double a0 = -f0, a1 = -f1, a2 = -f2;
-          const double d0 = a0 - a1, d1 = a1 - a2;
-          hits[0] |= (0.0 < f0 && f1 <= 0.0) ? 1u << i : 0u;
-          hits[1] |= (0.0 < a0 && a1 <= 0.0) ? 1u << i : 0u;
-          if (q_lo + i < peak_end) {
-            hits[2] |= (0.0 < d0 && d1 <= 0.0) ? 1u << i : 0u;
-            hits[3] |= (0.0 < -d0 && -d1 <= 0.0) ? 1u << i : 0u;
-          }
+      if (len > 0) {
+        unsigned long long pos, neg, up = 0, down = 0;
+        double prev = X(0);
+        {
+          const long long b = __double_as_longlong(prev);
+          pos = b > 0 ? 1ull : 0ull;
+          neg = static_cast<unsigned long long>(b) > 0x8000000000000000ull ? 1ull : 0ull;
         }
+        for (int i0 = 0; i0 <= len; i0 += 8) {
+          double v[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) v[u] = X(i0 + 1 + u);
+          unsigned gp = 0u, gn = 0u, gu = 0u, gd = 0u;
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const double cur = v[u];
+            const long long b = __double_as_longlong(cur);
+            gp |= (b > 0 ? 1u : 0u) << u;
+            gn |= (static_cast<unsigned long long>(b) > 0x8000000000000000ull ? 1u : 0u) << u;
+            gu |= (cur > prev ? 1u : 0u) << u;
+            gd |= (cur < prev ? 1u : 0u) << u;
+            prev = cur;
+          }
+          pos |= static_cast<unsigned long long>(gp) << (i0 + 1);
+          neg |= static_cast<unsigned long long>(gn) << (i0 + 1);
+          up |= static_cast<unsigned long long>(gu) << i0;
+          down |= static_cast<unsigned long long>(gd) << i0;
+        }
+        const unsigned len_mask = len >= 32 ? ~0u : (1u << len) - 1u;
+        const int pk = imax(0, imin(len, peak_end - q_lo));
+        const unsigned peak_mask = pk >= 32 ? ~0u : (1u << pk) - 1u;
+        hits[0] = static_cast<unsigned>(pos & ~(pos >> 1)) & len_mask;
+        hits[1] = static_cast<unsigned>(neg & ~(neg >> 1)) & len_mask;
+        hits[2] = static_cast<unsigned>(up & ~(up >> 1)) & peak_mask;
+        hits[3] = static_cast<unsigned>(down & ~(down >> 1)) & peak_mask;
       }
       const unsigned long long mine = static_cast<unsigned long long>(__popc(hits[0])) |
                                       static_cast<unsigned long long>(__popc(hits[1])) << 16 |
