@@ -121,6 +121,8 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
   const double fs = B.fs_r;
   const double half_rfs = 0.5 / fs, two_fs = 2.0 * fs;
   const double upper = centre * 1.1, lower = centre * 0.9;
+  // val > upper || val > ceil is val > min(upper, ceil); likewise below.
+  const double val_hi = fmin(upper, B.f0_ceil), val_lo = fmax(lower, B.f0_floor);
   int seg[4], last[4];
   double x0[4], x1[4], y0[4], y1[4], ea[4], eb[4];   // ea, eb: edges seg, seg + 1
   double inv[4];                                      // 1 / (x1 - x0)
@@ -195,7 +197,7 @@ __device__ inline void band_contour_walk(const BatchView& B, double* const ev[4]
       track[k] = y0[k] + s * (y1[k] - y0[k]);
     }
     double val = (track[0] + track[1] + track[2] + track[3]) / 4.0;
-    if (val > upper || val < lower || val > B.f0_ceil || val < B.f0_floor) val = 0.0;
+    if (val > val_hi || val < val_lo) val = 0.0;
     out[f] = val;
   }
 }
