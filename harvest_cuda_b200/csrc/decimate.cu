@@ -26,13 +26,12 @@ __device__ __forceinline__ void clip_of_segment(const DecimateView& v, int64_t s
   end = begin + v.seg_len < total ? begin + v.seg_len : total;
 }
 
-// Input of the forward pass at padded index i: the held and reflected clip.
-__device__ __forceinline__ double forward_input(const DecimateView& v, const double* x, int c,
-                                                int64_t i) {
-  int64_t n = v.x_off[c + 1] - v.x_off[c];
-  int64_t j = i - 9 - v.lag;
+// Input of the forward pass at padded index i: the held and reflected clip
+// (xc: the clip's samples, n of them).
+__device__ __forceinline__ double forward_input(const double* xc, int64_t n, int lag, int64_t i) {
+  int64_t j = i - 9 - lag;
   j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
-  return x[v.x_off[c] + j];
+  return xc[j];
 }
 
 // One step of FilterForDecimate (matlabfunctions.cpp:118-124); the expression
@@ -56,9 +55,12 @@ __global__ void decimate_segment_states(DecimateView v, const double* __restrict
   clip_of_segment(v, seg, c, begin, end);
   int64_t total = v.t_off[c + 1] - v.t_off[c];
   const double* uc = u + v.t_off[c];
+  const double* xc = x + v.x_off[c];
+  const int64_t n = v.x_off[c + 1] - v.x_off[c];
+  const int lag = v.lag;
   double s0 = 0.0, s1 = 0.0, s2 = 0.0;
   for (int64_t i = begin; i < end; ++i) {
-    double in = kPass == 0 ? forward_input(v, x, c, i) : uc[total - 1 - i];
+    double in = kPass == 0 ? forward_input(xc, n, lag, i) : uc[total - 1 - i];
     lowpass_step(v, in, s0, s1, s2);
   }
   states[3 * seg + 0] = s0;
@@ -113,7 +115,10 @@ __global__ void decimate_segment_run(DecimateView v, const double* __restrict__ 
   double* uc = u + v.t_off[c];
   double s0 = states[3 * seg], s1 = states[3 * seg + 1], s2 = states[3 * seg + 2];
   if (kPass == 0) {
-    for (int64_t i = begin; i < end; ++i) uc[i] = lowpass_step(v, forward_input(v, x, c, i), s0, s1, s2);
+    const double* xc = x + v.x_off[c];
+    const int64_t n = v.x_off[c + 1] - v.x_off[c];
+    const int lag = v.lag;
+    for (int64_t i = begin; i < end; ++i) uc[i] = lowpass_step(v, forward_input(xc, n, lag, i), s0, s1, s2);
     return;
   }
   // Kept sample k of the decimated clip sits at backward index
@@ -126,12 +131,18 @@ __global__ void decimate_segment_run(DecimateView v, const double* __restrict__ 
   int64_t y_len = v.y_off[c + 1] - v.y_off[c];
   int64_t anchor = total - 9 - nbeg;  // backward index of decimated sample 0
   double* yc = y + v.y_off[c];
+  // Kept indices j <= anchor with anchor - j a multiple of r, walked down
+  // from the last one: the first kept index at or after begin, then every
+  // r-th (one division per segment instead of one per sample).
+  int64_t keep = begin <= anchor ? begin + (anchor - begin) % r : end;
+  int64_t k = (anchor - keep) / r - skip;
+  const double* in = uc + (total - 1);
   for (int64_t j = begin; j < end; ++j) {
-    double out = lowpass_step(v, uc[total - 1 - j], s0, s1, s2);
-    int64_t dist = anchor - j;
-    if (dist >= 0 && dist % r == 0) {
-      int64_t k = dist / r - skip;
+    const double out = lowpass_step(v, in[-j], s0, s1, s2);
+    if (j == keep) {
       if (k >= 0 && k < y_len) yc[k] = out;
+      keep += r;
+      --k;
     }
   }
 }
