@@ -305,7 +305,7 @@ struct Plan {
   size_t arena_bytes = 0;
   struct Layout {
     size_t meta, pcm, x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores,
-        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed, keys, leaders;
+        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed, keys, leaders, item_off;
   } at{};
   int bank_ctas = 0;
   // Device pointers, set by Workspace::prepare: into the arena's copy of
@@ -663,6 +663,7 @@ struct Workspace {
     p->at.classes = take(sizeof(int) * (2 * kRefineClasses + 1));
     p->at.keys = take(sizeof(ulonglong2) * size_t(p->per_group) * F);
     p->at.leaders = take(2 * sizeof(unsigned long long) * size_t(p->per_group) * F);
+    p->at.item_off = take(sizeof(int64_t) * (size_t(B) + 1));
     p->at.refined = take(8 * size_t(p->capacity) * F);
     p->at.scores = take(8 * size_t(p->capacity) * F);
     p->at.pruned = take(8 * size_t(p->capacity) * F);
@@ -776,6 +777,7 @@ struct Workspace {
     rb.jobs = ptr<RefineJob>(p.at.jobs);
     rb.keys = ptr<ulonglong2>(p.at.keys);
     rb.leaders = ptr<unsigned long long>(p.at.leaders);
+    rb.item_off = ptr<int64_t>(p.at.item_off);
     rb.twiddles = twiddles;
     check(launch_refine(bv, rb, y, ptr<double>(p.at.cand), ptr<int>(p.at.count), F,
                         ptr<double>(p.at.refined), ptr<double>(p.at.scores), sms, p.refine_shape, s),
@@ -932,6 +934,7 @@ struct Workspace {
     rb.jobs = ptr<RefineJob>(p.at.jobs);
     rb.keys = ptr<ulonglong2>(p.at.keys);
     rb.leaders = ptr<unsigned long long>(p.at.leaders);
+    rb.item_off = ptr<int64_t>(p.at.item_off);
     rb.twiddles = twiddles;
     const int64_t F = p.frame_off[p.clips];
     RefineShape best{};

@@ -163,6 +163,7 @@ struct RefineBuffers {
   RefineJob* jobs;     // [frames * capacity]
   ulonglong2* keys;    // [frames * per_group] refinement key of every official candidate
   unsigned long long* leaders;  // [frames * per_group][2] job classes and sibling masks of the 7 overlap cells
+  int64_t* item_off;   // [clips + 1] bucket items (frame, official candidate) per clip, prefix
   const double2* twiddles;  // [kTwiddleN] e^{-2 pi i t / kTwiddleN}
 };
 // Launch shape of the refinement jobs: minimum resident 128-thread blocks per

@@ -78,16 +78,47 @@ __device__ __forceinline__ bool same_key(ulonglong2 a, ulonglong2 b) {
   return a.x == b.x && a.y == b.y && !(a.y >> 63);
 }
 
-__global__ void candidate_keys(BatchView v, const double* __restrict__ cand, int64_t slots,
-                               ulonglong2* __restrict__ keys) {
+// item_off[c] = sum over clips c' < c of frames(c') * count[c']: the items of
+// the bucket passes are the (frame, official candidate j < count) pairs,
+// numbered clip by clip, frame-major. One block; blockDim.x <= 256.
+__device__ void clip_item_offsets(const BatchView& v, const int* __restrict__ count,
+                                  int64_t* __restrict__ item_off) {
+  __shared__ long long part[256];
+  const int nt = blockDim.x, t = threadIdx.x;
+  const int per = (v.clips + nt - 1) / nt;
+  const int c0 = imin(t * per, v.clips), c1 = imin(c0 + per, v.clips);
+  long long sum = 0;
+  for (int c = c0; c < c1; ++c) sum += (v.frame_off[c + 1] - v.frame_off[c]) * count[c];
+  part[t] = sum;
+  __syncthreads();
+  for (int d = 1; d < nt; d <<= 1) {   // inclusive scan of the parts
+    const long long x = t >= d ? part[t - d] : 0;
+    __syncthreads();
+    part[t] += x;
+    __syncthreads();
+  }
+  long long run = part[t] - sum;
+  for (int c = c0; c < c1; ++c) {
+    item_off[c] = run;
+    run += (v.frame_off[c + 1] - v.frame_off[c]) * count[c];
+  }
+  if (t == nt - 1) item_off[v.clips] = part[t];
+}
+
+// Refinement keys of every official candidate slot; block 0 also writes the
+// bucket passes' item offsets.
+__global__ void candidate_keys(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
+                               int64_t slots, ulonglong2* __restrict__ keys, int64_t* __restrict__ item_off) {
+  if (blockIdx.x == 0) clip_item_offsets(v, count, item_off);
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= slots) return;
   const double f0c = cand[i];
   keys[i] = f0c > 0.0 ? refine_key(v.fs_r, f0c) : make_ulonglong2(0ull, 0ull);
 }
 
-// One thread per (frame, official candidate j): the seven overlap cells of
-// column j (groups g = 0..6) at this frame. A cell is a job when its
+// One thread per (frame, official candidate j < count) item (numbered by
+// item_off, so no lane waits on a column past its clip's count): the seven
+// overlap cells of column j (groups g = 0..6) at this frame. A cell is a job when its
 // candidate is nonzero and no lower group of the same j holds a candidate
 // with the same key; the leader's job also serves those later siblings.
 // Pass 1 (kScatter = false) finds the jobs, counts them per window-length
@@ -101,27 +132,41 @@ __global__ void candidate_keys(BatchView v, const double* __restrict__ cand, int
 template <bool kScatter>
 __global__ void __launch_bounds__(256)
 refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restrict__ count,
-              const ulonglong2* __restrict__ keys, int64_t total_frames, unsigned long long* __restrict__ leaders,
+              const ulonglong2* __restrict__ keys, const int64_t* __restrict__ item_off,
+              unsigned long long* __restrict__ leaders,
               int* __restrict__ class_count, int* __restrict__ class_cursor, RefineJob* __restrict__ jobs,
               double* __restrict__ refined, double* __restrict__ scores) {
   __shared__ int s_count[kRefineClasses], s_base[kRefineClasses];
   for (int i = threadIdx.x; i < kRefineClasses; i += blockDim.x) s_count[i] = 0;
   __syncthreads();
   const int64_t item = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const bool valid = item < total_frames * v.per_group;
+  const bool valid = item < item_off[v.clips];
+  // Clip, count, frame and column of the item (a clip with count 0 has no
+  // items, so K >= 1 here).
+  int c = 0, K = 1, f = 0, j = 0;
+  if (valid) {
+    c = owner(item_off, v.clips, item);
+    K = count[c];
+    const int64_t local = item - item_off[c];
+    if (local < 0x7fffffff) {
+      const int l = static_cast<int>(local);
+      f = l / K;
+      j = l - f * K;
+    } else {
+      f = static_cast<int>(local / K);
+      j = static_cast<int>(local - static_cast<int64_t>(f) * K);
+    }
+  }
+  const int64_t row0 = v.frame_off[c];
+  const int frames = static_cast<int>(v.frame_off[c + 1] - row0);
+  const int64_t gf = row0 + f;
   int cls[7], rank[7];
 #pragma unroll
   for (int g = 0; g < 7; ++g) cls[g] = -1;
   if (valid) {
     if (!kScatter) {
-      const int64_t gf = item / v.per_group;
-      const int j = static_cast<int>(item - gf * v.per_group);
-      const int c = owner(v.frame_off, v.clips, gf);
-      const int K = count[c];
       unsigned long long record = 0, sibling_record = 0;
-      if (j < K) {
-        const int64_t row0 = v.frame_off[c];
-        const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
+      {
         ulonglong2 key[7];
         bool live[7];
 #pragma unroll
@@ -180,12 +225,6 @@ refine_bucket(BatchView v, const double* __restrict__ cand, const int* __restric
 #pragma unroll
   for (int g = 0; g < 7; ++g) any |= cls[g] >= 0;
   if (!any) return;
-  const int64_t gf = item / v.per_group;
-  const int j = static_cast<int>(item - gf * v.per_group);
-  const int c = owner(v.frame_off, v.clips, gf);
-  const int K = count[c];
-  const int64_t row0 = v.frame_off[c];
-  const int frames = static_cast<int>(v.frame_off[c + 1] - row0), f = static_cast<int>(gf - row0);
   const unsigned long long sibling_record = leaders[2 * item + 1];
 #pragma unroll
   for (int g = 0; g < 7; ++g) {
@@ -516,11 +555,12 @@ cudaError_t launch_refine(const BatchView& v, const RefineBuffers& b, const doub
   if ((e = cudaMemsetAsync(b.class_count, 0, sizeof(int) * kRefineClasses, stream)) != cudaSuccess) return e;
   const int64_t slots = total_frames * v.per_group;
   const unsigned grid = static_cast<unsigned>((slots + 255) / 256);
-  candidate_keys<<<grid, 256, 0, stream>>>(v, cand, slots, b.keys);
-  refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.leaders, b.class_count,
+  candidate_keys<<<grid, 256, 0, stream>>>(v, cand, count, slots, b.keys, b.item_off);
+  // Items number at most frames * per_group, the slots.
+  refine_bucket<false><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, b.item_off, b.leaders, b.class_count,
                                                  b.class_cursor, b.jobs, refined, scores);
   refine_offsets<<<1, 32, 0, stream>>>(b.class_count, b.class_cursor, b.total);
-  refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, total_frames, b.leaders, b.class_count,
+  refine_bucket<true><<<grid, 256, 0, stream>>>(v, cand, count, b.keys, b.item_off, b.leaders, b.class_count,
                                                 b.class_cursor, b.jobs, refined, scores);
   const unsigned job_grid = static_cast<unsigned>(sms * shape.blocks_per_sm);
   auto kernel = shape.min_blocks == 4 ? refine_jobs<4> : (shape.min_blocks == 5 ? refine_jobs<5> : refine_jobs<1>);
