@@ -113,7 +113,8 @@ __global__ void candidate_keys(BatchView v, const double* __restrict__ cand, con
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= slots) return;
   const double f0c = cand[i];
-  keys[i] = f0c > 0.0 ? refine_key(v.fs_r, f0c) : make_ulonglong2(0ull, 0ull);
+  // Keys are read only for nonzero candidates (the bucket pass's live cells).
+  if (f0c > 0.0) keys[i] = refine_key(v.fs_r, f0c);
 }
 
 // One thread per (frame, official candidate j < count) item (numbered by

@@ -90,6 +90,44 @@ def test_long_voiced_section(gpu, checker, seconds, fs, period):
     assert np.max(np.abs(actual[0][both] - expected[0][both]) / expected[0][both]) <= 1e-10
 
 
+def _limit_cycle_period(x):
+    """Period of the state orbit of the smoothing filter (FilteringF0's
+    recursive part) on the constant input x from a zero state: 1 for a fixed
+    point, more for a rounding limit cycle."""
+    a0, a1 = 1.7347257688092754, -0.76600660094326412
+    w0 = w1 = 0.0
+    seen = {}
+    for k in range(3000):
+        if (w0, w1) in seen:
+            return k - seen[(w0, w1)]
+        seen[(w0, w1)] = k
+        w0, w1 = x + a0 * w0 + a1 * w1, w0
+    return 0
+
+
+def test_smoothing_of_held_limit_cycles(gpu, checker):
+    # Twenty voiced sections at different pitches. Each section is smoothed
+    # over the whole padded length with its first and last values held; on
+    # such a constant input the filter state ends in a fixed point or, for
+    # about a fifth of the values, in a rounding limit cycle, whose whole
+    # periods the engine skips. Its smoothed contour must equal the oracle's
+    # smoothing of the engine's own fixed contour bit for bit (all sections
+    # are shorter than 2048 frames).
+    fs, sections = 16000, 20
+    t = np.arange(int(fs * 0.3 * sections)) / fs
+    x = np.zeros_like(t)
+    for s in range(sections):
+        on = (t >= 0.3 * s) & (t < 0.3 * s + 0.18)
+        x[on] = sum(np.sin(2 * np.pi * (90.0 + 17.0 * s) * h * t[on]) / h for h in range(1, 6))
+    g = hv.api.stages(x, fs)
+    fixed = checker.fix_contour(g["pruned"], g["pruned_scores"], 7 * g["count"])
+    np.testing.assert_array_equal(g["smoothed"], checker.smooth_contour(fixed))
+    d = np.diff(np.concatenate([[0], (fixed > 0).astype(int), [0]]))
+    heads = fixed[np.flatnonzero(d == 1)]
+    assert len(heads) >= 15
+    assert sum(_limit_cycle_period(float(v)) > 1 for v in heads) >= 2
+
+
 def test_separate_voiced_sections(gpu, checker):
     fs = 16000
     t = np.arange(fs * 8) / fs
