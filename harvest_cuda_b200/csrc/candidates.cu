@@ -65,8 +65,9 @@ __global__ void official_candidates(BatchView v, const double* __restrict__ raw,
 // at 1 already covers), and packs this row's nonzero candidates, so that a
 // lane checks one of them at a time: about half of the 7 count columns are
 // zero, and with one lane per column the warp ran the minima once per 32
-// columns with most lanes idle. 5 capacity doubles of shared memory per
-// warp.
+// columns with most lanes idle. Per warp 2 capacity doubles and capacity
+// ints of shared memory (the packed columns; their values are re-read from
+// the row).
 __global__ void __launch_bounds__(128)
 prune_frames(BatchView v, const double* __restrict__ refined, const double* __restrict__ scores,
              const int* __restrict__ count, int64_t total_frames, double* __restrict__ pruned,
@@ -83,11 +84,9 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
   const int cap = v.capacity;
   const double* row = refined + gf * cap;
   const bool interior = f >= 1 && f <= frames - 2;
-  double* s_next = s_rows + (threadIdx.x >> 5) * 5 * cap;
+  double* s_next = s_rows + (threadIdx.x >> 5) * (2 * cap + (cap + 1) / 2);
   double* s_prev = s_next + cap;
-  double* s_ref = s_prev + cap;     // this row's candidates to check, packed
-  double* s_sc = s_ref + cap;
-  int* s_col = reinterpret_cast<int*>(s_sc + cap);
+  int* s_col = reinterpret_cast<int*>(s_prev + cap);   // this row's columns to check, packed
   const unsigned below = (1u << lane) - 1u;
   int n_next = 0, n_prev = 0, n_cur = 0;
   double top = 0.0, pick = 0.0;
@@ -120,10 +119,7 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
     const bool check = in && interior && ref != 0.0;
     const unsigned mc = __ballot_sync(0xffffffffu, check);
     if (check) {
-      const int k = n_cur + __popc(mc & below);
-      s_ref[k] = ref;
-      s_sc[k] = sc;
-      s_col[k] = j;
+      s_col[n_cur + __popc(mc & below)] = j;
     } else if (in) {
       pruned[gf * cap + j] = ref;
       pruned_scores[gf * cap + j] = sc;
@@ -133,8 +129,8 @@ prune_frames(BatchView v, const double* __restrict__ refined, const double* __re
   }
   __syncwarp();
   for (int k = lane; k < n_cur; k += 32) {
-    double ref = s_ref[k], sc = s_sc[k];
     const int col = s_col[k];
+    double ref = row[col], sc = scores[gf * cap + col];
     // SelectBestF0 leaves min(1, min_j |ref - c_j| / ref) as the error.
     // Correctly rounded division by the same positive ref is monotone, so
     // the smaller of the two rows' errors is the quotient of the smaller
@@ -169,9 +165,9 @@ cudaError_t launch_candidates(const BatchView& v, const double* raw, int64_t tot
 cudaError_t launch_prune(const BatchView& v, const double* refined, const double* scores,
                          const int* count, int64_t total_frames, double* pruned,
                          double* pruned_scores, double* best, cudaStream_t stream) {
-  // Up to 4 warps per block, each with 5 capacity doubles of shared memory,
-  // within the default 48 KB.
-  const size_t per_warp = 5 * sizeof(double) * static_cast<size_t>(v.capacity);
+  // Up to 4 warps per block, each with 2.5 capacity doubles of shared
+  // memory, within the default 48 KB.
+  const size_t per_warp = sizeof(double) * (2 * static_cast<size_t>(v.capacity) + (v.capacity + 1) / 2);
   const int warps = static_cast<int>(std::max<size_t>(1, std::min<size_t>(4, 49152 / per_warp)));
   prune_frames<<<static_cast<unsigned>((total_frames + warps - 1) / warps), 32 * warps, warps * per_warp, stream>>>(
       v, refined, scores, count, total_frames, pruned, pruned_scores, best);
