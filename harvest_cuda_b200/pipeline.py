@@ -4,7 +4,7 @@ previous batch's F0 travels back.
 
 ``harvest_batch`` (the NumPy API) does upload, compute and download in
 turn, so every call pays its own PCIe transfers on top of the compute (on
-the 256-clip 16 kHz batch: 209 MB up, 5 MB down, about 5 ms of a 61 ms
+the 256-clip 16 kHz batch: 209 MB up, 5 MB down, about 5 ms of a 49 ms
 call). A stream of batches (a corpus being analysed, a serving queue) can
 hide them: ``BatchPipeline.submit`` enqueues a batch and returns without
 waiting for the GPU, ``result`` returns the oldest outstanding batch's
