@@ -191,6 +191,7 @@ class ClockSampler:
         except Exception:           # no NVML binding or device: fall back to nvidia-smi
             nv = None
         if nv is not None:
+            self._nv = nv
             self.source = "nvml, 10 ms"
             self._stop = threading.Event()
 
@@ -217,6 +218,10 @@ class ClockSampler:
         if self.thread is not None:
             self._stop.set()
             self.thread.join(timeout=5)
+            try:
+                self._nv.nvmlShutdown()   # balances the nvmlInit of __enter__
+            except Exception:
+                pass
         if self.proc is not None:
             self.proc.terminate()
             try:

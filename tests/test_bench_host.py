@@ -31,6 +31,12 @@ def _fake_nvml(clocks, masks):
     nv.nvmlDeviceGetClockInfo = clock
     nv.nvmlDeviceGetMaxClockInfo = lambda h, kind: 1965
     nv.nvmlDeviceGetCurrentClocksEventReasons = reasons
+    nv.shutdowns = 0
+
+    def shutdown():
+        nv.shutdowns += 1
+
+    nv.nvmlShutdown = shutdown
     return nv
 
 
@@ -45,6 +51,7 @@ def test_clock_sampler_reads_nvml(monkeypatch):
     assert s["sm_max_mhz"] == 1965.0
     assert s["reasons"] == ["sw_power_cap"]
     assert 1950.0 <= s["sm_mhz"] <= 1965.0
+    assert nv.shutdowns == 1
 
 
 def test_clock_sampler_flags_throttling(monkeypatch):
