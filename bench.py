@@ -15,21 +15,28 @@ pass of the whole Harvest pipeline over that batch.
   overlapping each step's copies with its neighbours' compute;
   ``e2e.blocking`` is ``harvest_batch`` doing the three in turn.
 * ``per_clip``: the plain per-clip path (``harvest`` once per clip).
-* ``roofline``: the dominant kernel's algorithmic bytes per launch over its
-  CUDA-event duration (stage-timed steps) against the measured HBM copy
-  bandwidth, plus its algorithmic FP64 FLOP rate against the measured FP64
-  FMA peak.
+* ``roofline``: the band bank (the largest stage): its algorithmic FP64
+  FLOP rate (WORLD's FFT model) over its CUDA-event duration (stage-timed
+  steps) against the FP64 FMA throughput measured on the same GPU, the
+  stage's binding bound; beside it the stage-boundary byte rate against the
+  measured HBM copy bandwidth.
 * ``cpu_baseline``: the reference's bundled WORLD Harvest (oracle/_ref) on
-  the host cores over a bounded sample of the same batch.
-
+  the host cores over a bounded sample of the same batch (median of 3).
+* ``configs``: the other workloads (one 3 s clip at 16 kHz, one 60 s clip
+  at 44.1 kHz, 64 clips of 2-30 s at 48 kHz with 1 ms frames), each timed
+  the same way; single clips add the per-call latency of ``harvest()`` and
+  WORLD on one host core.
 * ``grad``: the F0 gradient (``harvest_cuda_b200.autograd``) on 32 clips of
   4 s at 16 kHz from the same generator, L = sum over voiced frames of
   (f0 - true f0)^2: forward + backward device milliseconds per audio second
   (CUDA events), and the agreement of dL/dx with central finite differences
   (eps 1e-6) at 64 random samples per clip.
 
-``--impl reference`` times that CPU implementation alone on the host cores
-and prints the same line with ``"impl": "reference"``.
+``--impl reference`` times that CPU implementation alone on every host core
+over every clip of the workload (the K timed steps together make one pass;
+median of three passes) and prints the same line with
+``"impl": "reference"``. It never loads the engine's library: the workload
+generator is loaded by path, not through the package.
 """
 from __future__ import annotations
 
@@ -65,8 +72,10 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="batch256_16k")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0,
-                    help="target duration of the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0,
+                    help="target duration of one pass of the CPU baseline sample (3 passes)")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip timing the other workloads (one 3 s clip, one 60 s clip, 64 clips at 48 kHz)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-per-clip", action="store_true")
     ap.add_argument("--no-grad", action="store_true", help="skip the F0-gradient measurement")
@@ -135,8 +144,24 @@ def byte_model(lengths, fs, floor, ceil, period):
 
 
 # ------------------------------------------------------------- workloads --
+def signals_module():
+    """``harvest_cuda_b200/signals.py`` loaded by its path. The generators
+    need only NumPy; importing them through the package would run its
+    ``__init__``, which loads the engine's shared library, and the reference
+    arm must not map that library."""
+    import importlib.util
+    name = "hv_bench_signals"
+    if name not in sys.modules:
+        spec = importlib.util.spec_from_file_location(
+            name, os.path.join(ROOT, "harvest_cuda_b200", "signals.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules[name] = mod
+        spec.loader.exec_module(mod)
+    return sys.modules[name]
+
+
 def make_workload(name, seed, clips=0):
-    from harvest_cuda_b200 import signals
+    signals = signals_module()
     wl = signals.workload(name, seed=seed)
     if clips:
         wl["clips"] = wl["clips"][:clips]
@@ -275,17 +300,47 @@ def cpu_sample(wl, target_seconds, cores):
     return chosen
 
 
-def run_cpu(pool, wl, clips):
+def run_cpu(pool, wl, clips, repeats=1):
+    """WORLD on `clips` of the workload, one clip per worker process, the
+    longest submitted first so that no core idles behind a long clip at the
+    end. Returns (audio seconds, median wall seconds over `repeats` passes,
+    checker kind, every pass's wall seconds)."""
     offs, x = wl["offsets"], wl["packed"]
+    order = sorted(clips, key=lambda i: offs[i] - offs[i + 1])
     tasks = [(np.ascontiguousarray(x[offs[i]:offs[i + 1]]), wl["fs"], wl["floor"], wl["ceil"],
-              wl["period"]) for i in clips]
-    t0 = time.perf_counter()
-    results = pool.map(_world_clip, tasks, chunksize=1)
-    wall = time.perf_counter() - t0
+              wl["period"]) for i in order]
+    walls = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        results = pool.map(_world_clip, tasks, chunksize=1)
+        walls.append(time.perf_counter() - t0)
     audio = sum(t[0].size for t in tasks) / wl["fs"]
     kind = "reference" if results and results[0][1] == "reference" else "port"
-    run_cpu.last_f0 = [r[2] for r in results]
-    return audio, wall, kind
+    by_clip = dict(zip(order, (r[2] for r in results)))
+    run_cpu.last_f0 = [by_clip[i] for i in clips]
+    return audio, statistics.median(walls), kind, walls
+
+
+def cpu_model():
+    """The host CPU's model name (from /proc/cpuinfo)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def mapped_libraries():
+    """Shared objects mapped into this process (from /proc/self/maps)."""
+    try:
+        with open("/proc/self/maps") as f:
+            return sorted({ln.split()[-1] for ln in f if ln.rstrip().endswith(".so") or ".so." in ln})
+    except OSError:
+        return []
 
 
 def accuracy_against(reference_f0, sample, f0, out_off, kind, device):
@@ -340,34 +395,47 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no F0 gradient"}), flush=True)
         return
     cores = os.cpu_count() or 1
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     wl = make_workload(args.workload, seed=1000, clips=args.clips)
+    offs = wl["offsets"]
+    every = list(range(len(offs) - 1))
     pool = mp.get_context("spawn").Pool(cores)
-    per_step = max(2.0, min(args.cpu_seconds, 150.0 / max(1, args.steps + args.warmup)))
-    clips = cpu_sample(wl, per_step, cores)
-    audio_total = wall_total = 0.0
-    kind = "port"
-    for step in range(args.warmup + args.steps):
-        audio, wall, kind = run_cpu(pool, wl, clips)
-        if step >= args.warmup:
-            audio_total += audio
-            wall_total += wall
+    # Warm-up steps: one of the shortest clips per worker (starts the
+    # workers and loads the library in each).
+    shortest = sorted(every, key=lambda i: offs[i + 1] - offs[i])[:cores]
+    for _ in range(args.warmup):
+        run_cpu(pool, wl, shortest)
+    # Timed: the K steps together are one pass over every clip of the
+    # workload (step k is the k-th K-th of the batch); the pass runs through
+    # one worker pool, longest clip first, so that no core idles at a step
+    # boundary. The pass is repeated three times and the median is reported.
+    repeats = 3
+    audio, wall, kind, walls = run_cpu(pool, wl, every, repeats=repeats)
     pool.close()
-    value = audio_total / wall_total
+    pool.join()
+    value = audio / wall
+    maps = mapped_libraries()
+    engine_maps = [m for m in maps if "libharvest_b200" in m]
+    if engine_maps:
+        raise RuntimeError(f"the reference arm mapped the engine's library: {engine_maps}")
+    base = {"value": value, "unit": "audio-s/s", "cores": cores, "cpu_model": cpu_model(),
+            "kind": kind, "repeats": repeats, "pass_walls_s": [round(w, 3) for w in walls],
+            "sample": f"every clip of the workload ({len(every)} clips, {audio:.1f} audio-s) per pass, "
+                      f"split over the {args.steps} timed steps, one clip per worker process "
+                      f"(WORLD is single-threaded), longest first; median of {repeats} passes"}
     line = {
         "impl": "reference", "metric": "batched audio-s/s (16 kHz)", "value": value,
         "unit": "audio-s/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * wall_total / args.steps, "higher_is_better": True,
+        "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
-                   "sample_clips": len(clips)},
-        "cpu_baseline": {"value": value, "unit": "audio-s/s", "cores": cores, "kind": kind,
-                         "sample": f"{len(clips)} clips ({audio_total / args.steps:.1f} audio-s) "
-                                   f"of the workload per step, one clip per worker process"},
+        "config": workload_config(args, wl, world),
+        "cpu_baseline": base,
         "e2e": {"value": value, "unit": "audio-s/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
     if not args.no_reference_cuda:
         line["reference_cuda"] = reference_cuda_measure(wl)
+    line["libraries_mapped"] = [m for m in mapped_libraries() if ROOT in m]
     print(json.dumps(line), flush=True)
 
 
@@ -550,22 +618,26 @@ def run_ours(args):
     line = None
     if rank == 0:
         line = summarize(args, wl, value, ms, stages, e2e, clocks.summary(), local, world)
-        line["config"]["autotuned"] = {"refine_min_blocks_per_sm": tuning[0], "refine_grid_blocks_per_sm": tuning[1],
-                                       "key": "fs, f0 range, log2 of the batch's samples"}
+        line["autotuned"] = {"refine_min_blocks_per_sm": tuning[0], "refine_grid_blocks_per_sm": tuning[1],
+                             "key": "fs, f0 range, log2 of the batch's samples"}
         if world == 1 and not args.no_per_clip:
             line["per_clip"] = per_clip(hv, wl, local)
             line["batched_over_per_clip"] = round(e2e["value"] / line["per_clip"]["value"], 2)
         if world == 1 and not args.no_grad:
             line["grad"] = grad_measure(hv, args.steps, max(3, args.warmup), stream,
                                         fd_per_clip=args.grad_fd_samples)
+        if world == 1 and not args.no_configs:
+            line["configs"] = {name: config_measure(hv, name, local, args.steps, args.warmup, stream, pool)
+                               for name in EXTRA_CONFIGS if name != args.workload}
         if pool is not None:
             sample = cpu_sample(wl, args.cpu_seconds, cores)
-            a, wall, kind = run_cpu(pool, wl, sample)
+            a, wall, kind, walls = run_cpu(pool, wl, sample, repeats=3)
             pool.close()
             line["cpu_baseline"] = {
-                "value": a / wall, "unit": "audio-s/s", "cores": cores, "kind": kind,
+                "value": a / wall, "unit": "audio-s/s", "cores": cores, "cpu_model": cpu_model(),
+                "kind": kind, "repeats": 3, "pass_walls_s": [round(w, 3) for w in walls],
                 "sample": f"{len(sample)} of the batch's clips ({a:.1f} audio-s), one clip per "
-                          f"worker process, {wall:.1f} s wall"}
+                          f"worker process, longest first; median of 3 passes, {wall:.1f} s wall"}
             line["accuracy"] = accuracy_against(run_cpu.last_f0, sample, f0, out_off, kind, local)
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -603,31 +675,48 @@ def ncu_traffic(stage, wl):
     return None if per is None else per * float(sum(wl["lengths"])) / wl["fs"]
 
 
-def summarize(args, wl, value, ms, stages, e2e, clocks, device, world):
+def workload_config(args, wl, world):
+    """The `config` object of the JSON line, shared by both arms so that
+    they describe the same workload the same way."""
+    return {"workload": args.workload, "description": WORKLOADS[args.workload],
+            "clips_per_gpu": len(wl["lengths"]),
+            "audio_seconds_per_gpu": float(sum(wl["lengths"])) / wl["fs"],
+            "l2": "inputs and working set larger than L2 (no flush)",
+            "parallelism": f"clip sharding, {world} GPU(s), no collective"}
+
+
+def roofline(wl, stages, device, traffic=True):
+    """The band bank's roofline: its algorithmic FP64 FLOP rate (WORLD's FFT
+    model) against the FP64 FMA throughput measured on this GPU, which is
+    the binding bound of the stage, and beside it the stage-boundary byte
+    rate against the measured HBM copy bandwidth."""
     hbm, hbm_src = load_peaks()
-    models = stage_models(wl)
-    dominant = max(stages, key=stages.get)
-    nbytes, flops = models[dominant]
-    dur = stages[dominant] / 1000.0
-    roof = {"bound": "hbm", "kernel": dominant, "achieved": nbytes / dur / 1e9, "peak": hbm,
-            "unit": "GB/s", "frac": nbytes / dur / 1e9 / hbm, "traffic": ncu_traffic(dominant, wl),
-            "peak_source": hbm_src, "algorithmic_bytes": nbytes, "launch_ms": stages[dominant]}
+    nbytes, flops = stage_models(wl)["band_bank"]
+    dur = stages["band_bank"] / 1000.0
     peak64 = fp64_peak(device)
-    if flops is not None and peak64:
-        roof["fp64"] = {"achieved": flops / dur / 1e12, "peak": peak64, "unit": "TFLOP/s",
-                        "frac": flops / dur / 1e12 / peak64, "algorithmic_flops": flops,
-                        "peak_source": "measured FMA loop (libhv_peaks)"}
+    hbm_part = {"hbm_achieved_gbs": nbytes / dur / 1e9, "hbm_peak_gbs": hbm,
+                "hbm_frac": nbytes / dur / 1e9 / hbm, "hbm_peak_source": hbm_src,
+                "algorithmic_bytes": nbytes}
+    common = {"kernel": "band_bank", "dominant_stage": max(stages, key=stages.get),
+              "launch_ms": stages["band_bank"],
+              "traffic": ncu_traffic("band_bank", wl) if traffic else None}
+    if peak64:
+        return {"bound": "fp64", "achieved": flops / dur / 1e12, "peak": peak64, "unit": "TFLOP/s",
+                "frac": flops / dur / 1e12 / peak64, "algorithmic_flops": flops,
+                "peak_source": "measured: FP64 FMA loop on this GPU (libhv_peaks)", **common, **hbm_part}
+    return {"bound": "hbm", "achieved": hbm_part["hbm_achieved_gbs"], "peak": hbm, "unit": "GB/s",
+            "frac": hbm_part["hbm_frac"], "peak_source": hbm_src, **common, **hbm_part}
+
+
+def summarize(args, wl, value, ms, stages, e2e, clocks, device, world):
+    roof = roofline(wl, stages, device)
     ratio = clip_params(int(wl["lengths"][0]), wl["fs"], wl["floor"], wl["ceil"])["ratio"]
     return {
         "metric": "batched audio-s/s (16 kHz)", "value": value, "unit": "audio-s/s",
         "n_gpus": world, "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
-                   "clips_per_gpu": len(wl["lengths"]),
-                   "audio_seconds_per_gpu": float(sum(wl["lengths"])) / wl["fs"],
-                   "l2": "inputs and working set larger than L2 (no flush)",
-                   "parallelism": f"clip sharding, {world} GPU(s), no collective"},
+        "config": workload_config(args, wl, world),
         "stage_ms": stages, "roofline": roof, "e2e": e2e, "clocks": clocks,
         "gpu_launches": kernels_per_step(ratio) * args.steps,
         "model_bytes_per_step": byte_model(wl["lengths"], wl["fs"], wl["floor"], wl["ceil"],
@@ -723,6 +812,110 @@ def grad_measure(hv, steps, warmup, stream, fd_per_clip=64, eps=1e-6):
         "audio_seconds": audio,
         "finite_differences": fd_report,
     }
+
+
+EXTRA_CONFIGS = ("clip3s_16k", "clip60s_44k", "batch64_48k")
+
+
+def config_measure(hv, name, device, steps, warmup, stream, pool):
+    """Another workload of the benchmark set, timed as the headline one:
+    device-resident steps through the C ABI (graph replay, CUDA events),
+    stage times, end to end from pinned host memory through BatchPipeline,
+    and the band bank's roofline. A single clip adds the per-call latency of
+    harvest() (host arrays in and out), and, with a worker pool, the
+    reference's WORLD on one host core (three single-threaded runs in
+    parallel processes, median) with the engine's agreement with it."""
+    import ctypes as ct
+    import torch
+    from harvest_cuda_b200 import _native
+    from harvest_cuda_b200.pipeline import BatchPipeline
+    wl = make_workload(name, seed=1000)
+    fs, floor, ceil, period = wl["fs"], wl["floor"], wl["ceil"], wl["period"]
+    offsets = np.ascontiguousarray(wl["offsets"], dtype=np.int64)
+    clips = offsets.size - 1
+    audio = float(offsets[-1]) / fs
+    out_off = hv.api._out_offsets(offsets, fs, period)
+    dev = torch.device("cuda", device)
+    x_dev = torch.from_numpy(wl["packed"]).to(dev)
+    f0_dev = torch.empty(int(out_off[-1]), dtype=torch.float64, device=dev)
+    t_dev = torch.empty_like(f0_dev)
+    off_ptr = offsets.ctypes.data_as(ct.POINTER(ct.c_int64))
+
+    def step(flags=0):
+        _native.raise_for(_native.lib.hv_harvest_batch(
+            x_dev.data_ptr(), off_ptr, clips, fs, floor, ceil, period, device, f0_dev.data_ptr(),
+            t_dev.data_ptr(), _native.HV_DEVICE_POINTERS | flags, stream.cuda_stream))
+
+    for _ in range(max(3, warmup)):
+        step()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        step()
+    end.record(stream)
+    torch.cuda.synchronize()
+    ms = start.elapsed_time(end) / steps
+    acc = np.zeros(_native.HV_STAGE_COUNT)
+    buf = np.zeros(_native.HV_STAGE_COUNT)
+    for _ in range(3):
+        step(_native.HV_RECORD_STAGES)
+        _native.raise_for(_native.lib.hv_last_stage_ms(buf.ctypes.data_as(ct.POINTER(ct.c_double))))
+        acc += buf
+    names = [_native.lib.hv_stage_name(i).decode() for i in range(_native.HV_STAGE_COUNT)]
+    stages = dict(zip(names, (acc / 3).round(4).tolist()))
+    pinned = torch.from_numpy(wl["packed"]).pin_memory()
+    x_host = pinned.numpy()
+    pipe = BatchPipeline(fs, floor, ceil, period, device=device, depth=2)
+    for _ in range(pipe.depth):
+        pipe.submit(x_host, offsets)
+    while pipe.pending():
+        pipe.result()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        pipe.submit(x_host, offsets)
+        if pipe.pending() == pipe.depth:
+            f0, times, _ = pipe.result()
+    while pipe.pending():
+        f0, times, _ = pipe.result()
+    e2e_s = (time.perf_counter() - t0) / steps
+    out = {"description": WORKLOADS[name], "clips": clips, "audio_seconds": audio,
+           "device_ms_per_step": ms, "value": audio / (ms / 1000.0), "unit": "audio-s/s",
+           "stage_ms": stages,
+           "e2e": {"value": audio / e2e_s, "unit": "audio-s/s", "ms_per_step": e2e_s * 1000.0,
+                   "h2d_bytes_per_step": int(x_host.nbytes),
+                   "d2h_bytes_per_step": int(f0.nbytes + times.nbytes),
+                   "api": "harvest_cuda_b200.pipeline.BatchPipeline (depth 2)"},
+           "roofline": roofline(wl, stages, device, traffic=False)}
+    if clips == 1:
+        x = np.ascontiguousarray(wl["packed"])
+        for _ in range(3):
+            hv.harvest(x, fs, floor, ceil, period, device=device)
+        laps = []
+        for _ in range(max(steps, 5)):
+            t0 = time.perf_counter()
+            f0, times = hv.harvest(x, fs, floor, ceil, period, device=device)
+            laps.append(time.perf_counter() - t0)
+        out["latency_ms"] = {"median": 1000.0 * statistics.median(laps), "min": 1000.0 * min(laps),
+                             "calls": len(laps),
+                             "api": "harvest_cuda_b200.harvest (NumPy in and out, one call per clip)"}
+        if pool is not None:
+            task = (x, fs, floor, ceil, period)
+            results = pool.map(_world_clip, [task] * 3, chunksize=1)
+            wall = statistics.median(r[0] for r in results)
+            ref = results[0][2]
+            both = (ref > 0) & (f0 > 0)
+            rel = np.abs(f0[both] - ref[both]) / ref[both]
+            out["cpu_single_thread"] = {
+                "value": audio / wall, "unit": "audio-s/s", "seconds_per_clip": wall, "cores": 1,
+                "cpu_model": cpu_model(), "kind": results[0][1], "repeats": 3,
+                "sample": "the whole clip; three single-threaded runs in parallel worker processes, median"}
+            out["accuracy"] = {"against": "WORLD Harvest (oracle/_ref)" if results[0][1] == "reference"
+                               else "C restatement (oracle)",
+                               "frames": int(ref.size),
+                               "vuv_disagreement": float(np.mean((ref > 0) != (f0 > 0))),
+                               "voiced_f0_rel_max": float(rel.max()) if rel.size else None}
+    return out
 
 
 def per_clip(hv, wl, device):

@@ -26,7 +26,7 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 SOURCES = ["decimate.cu", "bandbank.cu", "bandbank_fft.cu", "candidates.cu", "refine.cu", "contour.cu",
            "metrics.cu", "bank_adjoint.cu", "engine.cu"]
-HEADERS = ["hv_device.cuh", "hv_stages.cuh", "hv_events.cuh", "fft4096.cuh"]
+HEADERS = ["hv_device.cuh", "hv_stages.cuh", "hv_events.cuh", "fft4096.cuh", "hv_runtime.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-std=c++17", "-Xcompiler",
                 "-fPIC,-ffp-contract=off,-fvisibility=hidden", "-I" + INCLUDE]

@@ -355,6 +355,23 @@ cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, d
   return cudaGetLastError();
 }
 
+// Loads the module code of every kernel that launch_decimate, launch_copy
+// and launch_remove_mean start (lazy loading would otherwise load them, and
+// may allocate, at their first launch).
+cudaError_t preload_decimation_kernels() {
+  cudaFuncAttributes a;
+  cudaError_t e = cudaSuccess;
+  auto load = [&](const void* fn) { if (e == cudaSuccess) e = cudaFuncGetAttributes(&a, fn); };
+  load(reinterpret_cast<const void*>(decimate_segment_states<0>));
+  load(reinterpret_cast<const void*>(decimate_segment_states<1>));
+  load(reinterpret_cast<const void*>(decimate_chain));
+  load(reinterpret_cast<const void*>(decimate_segment_run<0>));
+  load(reinterpret_cast<const void*>(decimate_segment_run<1>));
+  load(reinterpret_cast<const void*>(copy_clips));
+  load(reinterpret_cast<const void*>(remove_mean_and_edge_bins));
+  return e;
+}
+
 cudaError_t launch_check_finite(const double* x, int64_t total, int* flag, int sms, cudaStream_t stream) {
   flag_nonfinite<<<sms * 4, 256, 0, stream>>>(x, total, flag);
   return cudaGetLastError();

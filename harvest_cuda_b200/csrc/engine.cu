@@ -1,10 +1,8 @@
 // Host engine and C ABI of the B200 Harvest engine.
 //
 //   * validation identical to the reference's bindings (src/bindings.cpp:18-39);
-//   * a per-device workspace cache whose clear() never invalidates a call in
-//     flight (src/workspace_cache.h:26-70);
-//   * primary-context handling that restores the caller's context
-//     (src/cuda_device.h:74-108);
+//   * the per-device workspace cache, device check and context handling of
+//     hv_runtime.h;
 //   * batch planning (parameters of src/engine.cpp:255-266 per clip), one
 //     device arena per workspace, and the launch sequence of the stages,
 //     captured once per batch shape into a CUDA graph and replayed.
@@ -28,6 +26,7 @@
 #include <vector>
 
 #include "harvest_b200.h"
+#include "hv_runtime.h"
 #include "hv_stages.cuh"
 
 namespace hv {
@@ -37,22 +36,6 @@ namespace {
 thread_local std::string g_error;
 thread_local double g_stage_ms[HV_STAGE_COUNT] = {};
 thread_local int g_tuning[3] = {0, 0, 0};   // refinement shape of the last call, and whether it tuned
-
-struct InvalidArgument : std::runtime_error { using std::runtime_error::runtime_error; };
-struct RuntimeFailure : std::runtime_error { using std::runtime_error::runtime_error; };
-
-void check(cudaError_t code, const char* what) {
-  if (code == cudaSuccess) return;
-  const char* name = cudaGetErrorName(code);
-  const char* text = cudaGetErrorString(code);
-  std::string msg = std::string("CUDA: ") + what + ": " + (name ? name : std::to_string(int(code)));
-  if (text) msg += std::string(": ") + text;
-  if (code == cudaErrorMemoryAllocation)
-    msg += ". GPU memory allocation failed; try shorter or fewer clips.";
-  if (code == cudaErrorNoDevice || code == cudaErrorInsufficientDriver)
-    msg += ". Check the NVIDIA driver and CUDA_VISIBLE_DEVICES.";
-  throw RuntimeFailure(msg);
-}
 
 template <class F>
 int guarded(F&& body) {
@@ -71,95 +54,6 @@ int guarded(F&& body) {
     return HV_RUNTIME_ERROR;
   }
 }
-
-// ------------------------------------------------- driver entry points --
-// Resolved through the runtime so the library has no link-time dependency
-// on libcuda (it loads on machines without a GPU driver).
-struct Driver {
-  decltype(&cuInit) init = nullptr;
-  decltype(&cuDevicePrimaryCtxRetain) retain = nullptr;
-  decltype(&cuDevicePrimaryCtxRelease) release = nullptr;
-  decltype(&cuCtxGetCurrent) get_current = nullptr;
-  decltype(&cuCtxSetCurrent) set_current = nullptr;
-  bool ok = false;
-  Driver() {
-    auto get = [](const char* name, void** fn) {
-      cudaDriverEntryPointQueryResult q;
-      return cudaGetDriverEntryPoint(name, fn, cudaEnableDefault, &q) == cudaSuccess && *fn &&
-             q == cudaDriverEntryPointSuccess;
-    };
-    ok = get("cuInit", reinterpret_cast<void**>(&init)) &&
-         get("cuDevicePrimaryCtxRetain", reinterpret_cast<void**>(&retain)) &&
-         get("cuDevicePrimaryCtxRelease", reinterpret_cast<void**>(&release)) &&
-         get("cuCtxGetCurrent", reinterpret_cast<void**>(&get_current)) &&
-         get("cuCtxSetCurrent", reinterpret_cast<void**>(&set_current));
-  }
-};
-const Driver& driver() {
-  static Driver d;
-  return d;
-}
-
-void check_device(int device) {
-  if (device < 0) throw InvalidArgument("device must be a nonnegative visible GPU index");
-  int count = 0;
-  cudaError_t e = cudaGetDeviceCount(&count);
-  if (e != cudaSuccess || count == 0) {
-    cudaGetLastError();
-    throw RuntimeFailure("CUDA: no usable GPU is visible (" +
-                         std::string(e == cudaSuccess ? "no devices" : cudaGetErrorString(e)) +
-                         "). Check the NVIDIA driver and CUDA_VISIBLE_DEVICES.");
-  }
-  if (device >= count)
-    throw InvalidArgument("device " + std::to_string(device) + " is out of range; " +
-                          std::to_string(count) + " GPU(s) are visible through CUDA_VISIBLE_DEVICES");
-  // One attribute query: cudaGetDeviceProperties fills every property
-  // through the driver and took milliseconds (at times over 100 ms) per call.
-  int major = 0;
-  check(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device), "cudaDeviceGetAttribute");
-  if (major < 10) {
-    cudaDeviceProp p{};
-    check(cudaGetDeviceProperties(&p, device), "cudaGetDeviceProperties");
-    throw RuntimeFailure("this build targets sm_100a (B200); device " + std::to_string(device) +
-                         " (" + p.name + ") has compute capability " + std::to_string(p.major) +
-                         "." + std::to_string(p.minor));
-  }
-}
-
-// Keeps a device's primary context retained while its workspace lives.
-class PrimaryContext {
- public:
-  explicit PrimaryContext(int device) : device_(device) {
-    const Driver& d = driver();
-    if (!d.ok) throw RuntimeFailure("CUDA driver entry points unavailable");
-    if (d.init(0) != CUDA_SUCCESS) throw RuntimeFailure("cuInit failed");
-    if (d.retain(&ctx_, device) != CUDA_SUCCESS) throw RuntimeFailure("cuDevicePrimaryCtxRetain failed");
-  }
-  ~PrimaryContext() { driver().release(device_); }
-  CUcontext get() const { return ctx_; }
-
- private:
-  int device_;
-  CUcontext ctx_ = nullptr;
-};
-
-// Makes `target` current and restores the caller's context on exit.
-class ContextGuard {
- public:
-  explicit ContextGuard(CUcontext target) {
-    const Driver& d = driver();
-    if (d.get_current(&prev_) != CUDA_SUCCESS) throw RuntimeFailure("cuCtxGetCurrent failed");
-    switched_ = prev_ != target;
-    if (switched_ && d.set_current(target) != CUDA_SUCCESS) throw RuntimeFailure("cuCtxSetCurrent failed");
-  }
-  ~ContextGuard() {
-    if (switched_) driver().set_current(prev_);
-  }
-
- private:
-  CUcontext prev_ = nullptr;
-  bool switched_ = false;
-};
 
 // ------------------------------------------------------------- WORLD maths --
 constexpr double kLog2 = 0.69314718055994529;  // world::kLog2
@@ -349,6 +243,9 @@ struct DeviceBank {
 
 constexpr int kSegment = 256;   // decimation scan segment length
 
+// Edge padding of GetWaveformAndSpectrumSub (harvest.cpp:50-51): ceil(140 / r) r samples.
+constexpr int decimation_lag(int ratio) { return (140 + ratio - 1) / ratio * ratio; }
+
 void mat3_mul(const double* a, const double* b, double* out) {
   double r[9];
   for (int i = 0; i < 3; ++i)
@@ -365,8 +262,7 @@ struct Workspace {
   cudaStream_t stream = nullptr;
   cudaEvent_t marks[HV_STAGE_COUNT + 1] = {};
   cudaEvent_t last = nullptr;  // completion of the previous call's work
-  void* arena = nullptr;
-  size_t arena_size = 0;
+  GrowingBuffer arena;          // the plans' device arena
   int sms = 0;
   double2* twiddles = nullptr;  // e^{-2 pi i t / 8192}, t < 8192
   int* host_flag = nullptr;      // pinned word for the non-finite-sample flag
@@ -378,10 +274,8 @@ struct Workspace {
   std::map<Settings, std::unique_ptr<DeviceBank>> device_banks;
   uint64_t next_plan_id = 1;
   uint64_t meta_owner = 0;   // plan whose tables are at the head of the arena
-  void* metric_buf = nullptr;   // inputs and offsets of hv_compare_batch
-  size_t metric_size = 0;
-  void* raw_buf = nullptr;      // band-bank dump and adjoint scratch of the per-band-candidate gradient
-  size_t raw_size = 0;
+  GrowingBuffer metric_buf;     // inputs and offsets of hv_compare_batch
+  GrowingBuffer raw_buf;        // band-bank dump and adjoint scratch of the per-band-candidate gradient
 
   explicit Workspace(int dev) : device(dev), ctx(dev) {
     ContextGuard g(ctx.get());
@@ -401,9 +295,9 @@ struct Workspace {
       if (stream) cudaStreamSynchronize(stream);
       plans.clear();
       device_banks.clear();
-      if (arena) cudaFree(arena);
-      if (metric_buf) cudaFree(metric_buf);
-      if (raw_buf) cudaFree(raw_buf);
+      arena.release();
+      metric_buf.release();
+      raw_buf.release();
       if (twiddles) cudaFree(twiddles);
       if (host_flag) cudaFreeHost(host_flag);
       for (auto& e : marks) if (e) cudaEventDestroy(e);
@@ -414,21 +308,13 @@ struct Workspace {
   }
 
   void ensure_arena(size_t bytes) {
-    if (bytes <= arena_size) return;
-    check(cudaEventSynchronize(last), "cudaEventSynchronize");
-    check(cudaStreamSynchronize(stream), "cudaStreamSynchronize");
-    if (arena) cudaFree(arena);
-    arena = nullptr;
-    arena_size = 0;
+    if (bytes <= arena.size) return;
+    // Graphs captured the old arena's addresses.
     for (auto& p : plans) {
       if (p->graph) { cudaGraphExecDestroy(p->graph); p->graph = nullptr; }
     }
-    // Headroom of min(size, 512 MB): a run of calls with growing lengths
-    // reallocates a few times, and a large batch adds little on top.
-    size_t grow = bytes + std::min<size_t>(bytes, size_t(512) << 20);
     meta_owner = 0;
-    check(cudaMalloc(&arena, grow), "cudaMalloc(workspace)");
-    arena_size = grow;
+    arena.reserve(bytes, last, stream, true, "cudaMalloc(workspace)");
   }
 
   // The device band tables of `s`, with filter spectra when `spectra`.
@@ -551,7 +437,7 @@ struct Workspace {
     p->capacity = p->per_group * 7;
     if (p->capacity >= kRefineColumns)
       throw InvalidArgument("f0_floor/f0_ceil span too many band-pass channels");
-    p->lag = static_cast<int>(std::ceil(140.0 / p->ratio) * p->ratio);
+    p->lag = decimation_lag(p->ratio);
     const double first = p->bank->centre[0];
     p->x_off.assign(B + 1, 0); p->y_off.assign(B + 1, 0); p->t_off.assign(B + 1, 0);
     p->seg_off.assign(B + 1, 0); p->frame_off.assign(B + 1, 0); p->out_off.assign(B + 1, 0);
@@ -680,7 +566,7 @@ struct Workspace {
   }
 
   template <class T>
-  T* ptr(size_t at) const { return reinterpret_cast<T*>(static_cast<char*>(arena) + at); }
+  T* ptr(size_t at) const { return reinterpret_cast<T*>(static_cast<char*>(arena.ptr) + at); }
 
   static BatchView batch_view(const Plan& p) {
     BatchView bv{};
@@ -812,16 +698,8 @@ struct Workspace {
     const size_t gradf_n = size_t(p.bands) * size_t(y_total);
     const size_t slot_n = size_t(ctas) * 4 * size_t(p.slot_capacity);
     const size_t need = align_up(8 * dump_n) + align_up(8 * gradf_n) + 3 * align_up(8 * slot_n);
-    if (need > raw_size) {
-      check(cudaEventSynchronize(last), "cudaEventSynchronize");
-      check(cudaStreamSynchronize(s), "cudaStreamSynchronize");
-      if (raw_buf) cudaFree(raw_buf);
-      raw_buf = nullptr;
-      raw_size = 0;
-      check(cudaMalloc(&raw_buf, need), "cudaMalloc(raw gradient)");
-      raw_size = need;
-    }
-    char* m = static_cast<char*>(raw_buf);
+    raw_buf.reserve(need, last, s, false, "cudaMalloc(raw gradient)");
+    char* m = static_cast<char*>(raw_buf.ptr);
     double* dump = reinterpret_cast<double*>(m);
     double* grad_f = reinterpret_cast<double*>(m + align_up(8 * dump_n));
     char* slots = m + align_up(8 * dump_n) + align_up(8 * gradf_n);
@@ -970,7 +848,7 @@ struct Workspace {
       enqueue(p, s, marks_on);
       return;
     }
-    if (!p.graph || p.graph_arena != arena) {
+    if (!p.graph || p.graph_arena != arena.ptr) {
       if (p.graph) { cudaGraphExecDestroy(p.graph); p.graph = nullptr; }
       cudaGraph_t g = nullptr;
       check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
@@ -985,59 +863,17 @@ struct Workspace {
       cudaError_t e = cudaGraphInstantiate(&p.graph, g, 0);
       cudaGraphDestroy(g);
       check(e, "cudaGraphInstantiate");
-      p.graph_arena = arena;
+      p.graph_arena = arena.ptr;
     }
     check(cudaGraphLaunch(p.graph, s), "cudaGraphLaunch");
   }
 };
 
-// One workspace per device behind a lease; clear() retires them without
-// invalidating leases in flight (same contract as the reference's cache).
-class WorkspaceCache {
-  struct Slot {
-    std::mutex mutex;
-    std::unique_ptr<Workspace> ws;
-  };
-  std::mutex mutex_;
-  std::map<int, std::shared_ptr<Slot>> slots_;
-  uint64_t generation_ = 0;
-
- public:
-  class Lease {
-    std::shared_ptr<Slot> slot_;
-    std::unique_lock<std::mutex> lock_;
-
-   public:
-    Lease(WorkspaceCache& cache, int device) {
-      uint64_t gen;
-      {
-        std::lock_guard<std::mutex> l(cache.mutex_);
-        gen = cache.generation_;
-        auto it = cache.slots_.find(device);
-        if (it != cache.slots_.end()) slot_ = it->second;
-      }
-      if (!slot_) {
-        auto created = std::make_shared<Slot>();
-        created->ws = std::make_unique<Workspace>(device);
-        std::lock_guard<std::mutex> l(cache.mutex_);
-        slot_ = gen == cache.generation_ ? cache.slots_.try_emplace(device, created).first->second : created;
-      }
-      lock_ = std::unique_lock<std::mutex>(slot_->mutex);
-    }
-    Workspace& get() const { return *slot_->ws; }
-  };
-  void clear() {
-    std::map<int, std::shared_ptr<Slot>> retired;
-    {
-      std::lock_guard<std::mutex> l(mutex_);
-      ++generation_;
-      retired.swap(slots_);
-    }
-  }
-};
+using WorkspaceCache = DeviceCache<Workspace>;
 
 WorkspaceCache& cache() {
-  static WorkspaceCache* c = new WorkspaceCache();  // outlives static teardown order
+  // Never destroyed: leases may end during static teardown.
+  static WorkspaceCache* c = new WorkspaceCache([](int device) { return std::make_unique<Workspace>(device); });
   return *c;
 }
 
@@ -1106,11 +942,20 @@ void validate_batch(const int64_t* offsets, int clips, int fs, double f0_floor, 
 // Scratch of hv_decimate_noalloc: a fixed array in the library's device
 // image, present on every GPU that loads the library for the life of the
 // process. It holds the forward low-pass pass (n + 2 lag + 18 doubles), the
-// segment states (3 per 256 samples), the clip offsets and two spare words.
+// segment states (3 per 256 samples) and a 16-word tail: the offset tables
+// (words 0-7), the FFT size (word 8) and the three edge bins (words 10-12)
+// that the DC-removal kernel writes.
+constexpr int max_decimation_lag() {
+  int m = 0;
+  for (int r = 2; r <= 12; ++r) m = decimation_lag(r) > m ? decimation_lag(r) : m;
+  return m;
+}
+constexpr int kNoAllocMaxLag = 144;
+static_assert(max_decimation_lag() == kNoAllocMaxLag, "largest decimation lag over ratios 2-12");
 constexpr int64_t kNoAllocMaxSamples = int64_t(1) << 20;
-constexpr int64_t kNoAllocPadded = kNoAllocMaxSamples + 2 * 151 + 18;   // lag <= 151
+constexpr int64_t kNoAllocPadded = kNoAllocMaxSamples + 2 * kNoAllocMaxLag + 18;
 constexpr int64_t kNoAllocSegments = (kNoAllocPadded + kSegment - 1) / kSegment;
-constexpr int64_t kNoAllocMeta = 16;                                      // offsets, nfft, bins
+constexpr int64_t kNoAllocMeta = 16;
 constexpr int64_t kNoAllocDoubles = kNoAllocPadded + 3 * kNoAllocSegments + kNoAllocMeta;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
@@ -1124,21 +969,38 @@ __global__ void noalloc_tables(int64_t* meta, int64_t n, int64_t y_len, int64_t 
   reinterpret_cast<int*>(meta + 8)[0] = nfft;
 }
 
-// Device address of the scratch per device, resolved once with that device's
-// primary context current.
+// Per device: the retained primary context and the scratch's device address,
+// set up once by the first call on that device (with that device's context
+// current), which also loads every kernel the entry point launches so that
+// later calls do not load module code (which may allocate). A failed set-up
+// is not remembered: the next call tries again.
 struct NoAllocDevice {
   std::once_flag once;
   std::unique_ptr<PrimaryContext> ctx;
   double* scratch = nullptr;
-  cudaError_t status = cudaSuccess;
 };
 NoAllocDevice& noalloc_device(int device) {
   static std::mutex mutex;
-  static std::map<int, std::unique_ptr<NoAllocDevice>> devices;
+  // Never destroyed: releasing primary contexts during static teardown may
+  // run after the CUDA driver has shut down.
+  static auto* devices = new std::map<int, std::unique_ptr<NoAllocDevice>>();
   std::lock_guard<std::mutex> lock(mutex);
-  auto& slot = devices[device];
+  auto& slot = (*devices)[device];
   if (!slot) slot = std::make_unique<NoAllocDevice>();
   return *slot;
+}
+
+void noalloc_setup(NoAllocDevice& dev, int device) {
+  auto ctx = std::make_unique<PrimaryContext>(device);
+  ContextGuard g(ctx->get());
+  void* address = nullptr;
+  check(cudaGetSymbolAddress(&address, g_noalloc_scratch), "cudaGetSymbolAddress(scratch)");
+  if (!address) throw RuntimeFailure("device scratch unavailable");
+  cudaFuncAttributes attr;
+  check(cudaFuncGetAttributes(&attr, reinterpret_cast<const void*>(noalloc_tables)), "load noalloc_tables");
+  check(preload_decimation_kernels(), "load decimation kernels");
+  dev.scratch = static_cast<double*>(address);
+  dev.ctx = std::move(ctx);
 }
 
 }  // namespace
@@ -1316,16 +1178,9 @@ int hv_compare_batch(const double* reference, const double* f0, const int64_t* o
     const size_t track_bytes = on_device ? 0 : align_up(8 * size_t(total));
     const size_t stat_bytes = on_device ? 0 : align_up(8 * 7 * size_t(clips));
     const size_t need = off_bytes + 2 * track_bytes + stat_bytes;
-    if (need > ws.metric_size) {
-      check(cudaEventSynchronize(ws.last), "cudaEventSynchronize");
-      if (ws.metric_buf) cudaFree(ws.metric_buf);
-      ws.metric_buf = nullptr;
-      ws.metric_size = 0;
-      check(cudaMalloc(&ws.metric_buf, need), "cudaMalloc(metrics)");
-      ws.metric_size = need;
-    }
+    ws.metric_buf.reserve(need, ws.last, st, false, "cudaMalloc(metrics)");
     check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
-    char* m = static_cast<char*>(ws.metric_buf);
+    char* m = static_cast<char*>(ws.metric_buf.ptr);
     std::vector<int64_t> rel(clips + 1);
     for (int c = 0; c <= clips; ++c) rel[c] = offsets[c] - base;
     int64_t* d_off = reinterpret_cast<int64_t*>(m);
@@ -1481,19 +1336,12 @@ int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* 
     if (!x || !y) throw InvalidArgument("null buffer");
     check_device(device);
     NoAllocDevice& dev = noalloc_device(device);
-    std::call_once(dev.once, [&] {
-      dev.ctx = std::make_unique<PrimaryContext>(device);
-      ContextGuard g(dev.ctx->get());
-      void* address = nullptr;
-      dev.status = cudaGetSymbolAddress(&address, g_noalloc_scratch);
-      dev.scratch = static_cast<double*>(address);
-    });
-    check(dev.status, "cudaGetSymbolAddress(scratch)");
-    if (!dev.scratch) throw RuntimeFailure("device scratch unavailable");
+    // An exception leaves the once_flag unset, so a failed set-up is retried.
+    std::call_once(dev.once, [&] { noalloc_setup(dev, device); });
     ContextGuard guard(dev.ctx->get());
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const int64_t y_len = (n + ratio - 1) / ratio;
-    const int lag = static_cast<int>(std::ceil(140.0 / ratio) * ratio);
+    const int lag = decimation_lag(ratio);
     const int64_t padded = ratio > 1 ? n + 2 * lag + 18 : 0;
     const int64_t segments = ratio > 1 ? (padded + kSegment - 1) / kSegment : 0;
     double* u = dev.scratch;
@@ -1502,9 +1350,10 @@ int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* 
     double* bins = reinterpret_cast<double*>(meta + 10);
     noalloc_tables<<<1, 1, 0, s>>>(meta, n, y_len, padded, segments, static_cast<int>(2 * y_len));
     check(cudaGetLastError(), "noalloc_tables");
+    // The DC removal reads only y_off and nfft of its batch view.
     BatchView bv{};
     bv.clips = 1; bv.ratio = ratio; bv.fs_r = double(fs) / ratio;
-    bv.x_off = meta; bv.y_off = meta + 2; bv.frame_off = meta + 2;
+    bv.x_off = meta; bv.y_off = meta + 2;
     bv.nfft = reinterpret_cast<const int*>(meta + 8);
     if (ratio > 1) {
       DecimateView dv{};

@@ -86,6 +86,7 @@ struct GradView {
 cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, double* states,
                             int64_t segments, double* y, cudaStream_t stream);
 cudaError_t launch_copy(const double* x, int64_t total, double* y, cudaStream_t stream);
+cudaError_t preload_decimation_kernels();
 cudaError_t launch_compare(const double* ref, const double* f0, const int64_t* off, int clips, double* stats,
                            cudaStream_t stream);
 cudaError_t launch_pcm16(const int16_t* in, int64_t total, double* out, int sms, cudaStream_t stream);

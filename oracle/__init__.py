@@ -134,6 +134,29 @@ def best():
     return reference() or port()
 
 
+def _harvest_task(args):
+    x, fs, f0_floor, f0_ceil, frame_period = args
+    return best().harvest(x, fs, f0_floor, f0_ceil, frame_period)
+
+
+def harvest_many(clips, fs, f0_floor=71.0, f0_ceil=800.0, frame_period=5.0, processes=None):
+    """``best().harvest`` on every clip, one clip per worker process (WORLD
+    is single-threaded), longest clip first. The workers are spawned, not
+    forked, so this is safe in a process that has already used CUDA.
+    Returns ``(f0, times)`` pairs in clip order."""
+    import multiprocessing as mp
+    order = sorted(range(len(clips)), key=lambda i: -len(clips[i]))
+    tasks = [(np.ascontiguousarray(clips[i], dtype=np.float64), int(fs), float(f0_floor),
+              float(f0_ceil), float(frame_period)) for i in order]
+    workers = max(1, min(len(tasks), processes or os.cpu_count() or 1))
+    with mp.get_context("spawn").Pool(workers) as pool:
+        results = pool.map(_harvest_task, tasks, chunksize=1)
+    out = [None] * len(clips)
+    for i, r in zip(order, results):
+        out[i] = r
+    return out
+
+
 class ReferenceCuda:
     """The reference's own GPU Harvest (one clip per call, as its API)."""
 
