@@ -59,6 +59,8 @@ SIGNATURES = {
                                      ct.c_void_p, ct.c_void_p]),
     "hv_raw_candidates_backward": (ct.c_int, [ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
                                               ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p]),
+    "hv_contour_batch": (ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, _L, ct.c_int, ct.c_int, ct.c_int,
+                                    ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_uint, ct.c_void_p]),
     "hv_clear_cache": (ct.c_int, []),
 }
 

@@ -161,6 +161,39 @@ def stages(x, fs, f0_floor=71.0, f0_ceil=800.0, *, device=0):
     return out
 
 
+def contour_batch(f0_candidates, scores, frame_offsets, columns=None, base=None, *, device=0):
+    """FixF0Contour and SmoothF0Contour of the engine's contour stage on
+    caller-given candidates (see ``hv_contour_batch``). ``f0_candidates``
+    and ``scores`` are float64 ``[frames, stride]`` arrays holding every
+    clip's rows back to back, ``frame_offsets`` (clips + 1 entries, from 0)
+    delimits the clips, and the first ``columns`` columns (default: all) are
+    the candidates. ``base`` (float64 ``[frames]``) replaces SearchF0Base's
+    contour as the input of FixStep1. Returns ``(fixed, smoothed)``."""
+    cand = np.ascontiguousarray(f0_candidates, dtype=np.float64)
+    sc = np.ascontiguousarray(scores, dtype=np.float64)
+    if cand.ndim != 2 or sc.shape != cand.shape:
+        raise ValueError("f0_candidates and scores must be 2-D arrays of the same shape")
+    frames, stride = cand.shape
+    if stride == 0:        # no candidate columns: one zero column keeps the rows addressable
+        cand, sc, stride, columns = np.zeros((frames, 1)), np.zeros((frames, 1)), 1, 0
+    columns = stride if columns is None else _as_int(columns, "columns")
+    off = np.ascontiguousarray(frame_offsets, dtype=np.int64)
+    if off.ndim != 1 or off.size < 2 or off[0] != 0 or off[-1] != frames:
+        raise ValueError("frame_offsets must run from 0 to the number of rows")
+    b = None
+    if base is not None:
+        b = np.ascontiguousarray(base, dtype=np.float64)
+        if b.shape != (frames,):
+            raise ValueError("base must hold one value per row")
+    fixed, smoothed = np.zeros(frames), np.zeros(frames)
+    status = _native.lib.hv_contour_batch(
+        cand.ctypes.data, sc.ctypes.data, None if b is None else b.ctypes.data,
+        off.ctypes.data_as(ct.POINTER(ct.c_int64)), off.size - 1, columns, stride,
+        _as_int(device, "device"), fixed.ctypes.data, smoothed.ctypes.data, 0, None)
+    _native.raise_for(status)
+    return fixed, smoothed
+
+
 def _out_offsets(offsets, fs, frame_period):
     lens = [output_length(int(offsets[i + 1] - offsets[i]), fs, frame_period)
             for i in range(len(offsets) - 1)]

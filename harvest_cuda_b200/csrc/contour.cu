@@ -434,7 +434,7 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
   const BatchView& B = v.batch;
   const int64_t row0 = B.frame_off[c];
   const int F = static_cast<int>(B.frame_off[c + 1] - row0);
-  const int columns = 7 * v.count[c];
+  const int columns = v.column_multiple * v.count[c];
   const int stride = B.capacity;
   const double* cand = v.pruned + row0 * stride;
   const double* score = v.pruned_scores + row0 * stride;
@@ -618,6 +618,8 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
     for (int j = bl[2 * i + 1] + 1; j <= bl[2 * (i + 1)] - 1; ++j) s4[j] = v0 + slope * cnt++;
   }
   __syncwarp();
+  if (v.fixed_out)
+    for (int i = lane; i < F; i += 32) v.fixed_out[row0 + i] = s4[i];
   // SmoothF0Contour (harvest.cpp:1079-1113), one voiced section per lane.
   double* sm = v.smoothed + row0;
   for (int i = lane; i < F; i += 32) sm[i] = 0.0;
@@ -649,6 +651,7 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
       smooth_section_warp(padded, bl[2 * s], bl[2 * s + 1], len, sm, shared_tail, len);
   // Resampling (harvest.cpp:1246-1251); for frame_period 1 the same
   // expression reproduces the direct branch (harvest.cpp:1230-1235).
+  if (!v.f0_out) return;
   const int64_t o0 = v.out_off[c];
   const int out_len = static_cast<int>(v.out_off[c + 1] - o0);
   for (int i = lane; i < out_len; i += 32) {
@@ -798,6 +801,36 @@ cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream) {
 
 cudaError_t launch_contour(const ContourView& v, cudaStream_t stream) {
   contour_clips<<<v.batch.clips, 32, 0, stream>>>(v);
+  return cudaGetLastError();
+}
+
+// SearchF0Base (harvest.cpp:693-705) per frame: the candidate of the first
+// highest score strictly above zero (a NaN score never wins), else 0. One
+// thread per frame; rows are [frames][stride], clip c has columns[c].
+__global__ void search_base(const double* __restrict__ cand, const double* __restrict__ scores,
+                            int64_t total_frames, int stride, const int64_t* __restrict__ frame_off, int clips,
+                            const int* __restrict__ columns, double* __restrict__ base) {
+  const int64_t f = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  if (f >= total_frames) return;
+  const int cols = columns[owner(frame_off, clips, f)];
+  const double* c = cand + f * stride;
+  const double* s = scores + f * stride;
+  double best = 0.0, best_score = 0.0;
+  for (int j = 0; j < cols; ++j)
+    if (s[j] > best_score) {
+      best = c[j];
+      best_score = s[j];
+    }
+  base[f] = best;
+}
+
+cudaError_t launch_search_base(const double* cand, const double* scores, int64_t total_frames, int stride,
+                               const int64_t* frame_off, int clips, const int* columns, double* base,
+                               cudaStream_t stream) {
+  if (total_frames <= 0) return cudaSuccess;
+  const int threads = 256;
+  search_base<<<static_cast<unsigned>((total_frames + threads - 1) / threads), threads, 0, stream>>>(
+      cand, scores, total_frames, stride, frame_off, clips, columns, base);
   return cudaGetLastError();
 }
 

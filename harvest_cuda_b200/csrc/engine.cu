@@ -276,6 +276,7 @@ struct Workspace {
   uint64_t meta_owner = 0;   // plan whose tables are at the head of the arena
   GrowingBuffer metric_buf;     // inputs and offsets of hv_compare_batch
   GrowingBuffer raw_buf;        // band-bank dump and adjoint scratch of the per-band-candidate gradient
+  GrowingBuffer contour_buf;    // tables, copies and scratch of hv_contour_batch
 
   explicit Workspace(int dev) : device(dev), ctx(dev) {
     ContextGuard g(ctx.get());
@@ -298,6 +299,7 @@ struct Workspace {
       arena.release();
       metric_buf.release();
       raw_buf.release();
+      contour_buf.release();
       if (twiddles) cudaFree(twiddles);
       if (host_flag) cudaFreeHost(host_flag);
       for (auto& e : marks) if (e) cudaEventDestroy(e);
@@ -611,6 +613,8 @@ struct Workspace {
     cv.scratch_off = p.d_scratch_off; cv.scratch = ptr<double>(p.at.scratch);
     cv.smoothed = ptr<double>(p.at.smoothed); cv.period = p.s.period; cv.out_off = p.d_out_off;
     cv.f0_out = ptr<double>(p.at.f0); cv.t_out = ptr<double>(p.at.times);
+    cv.column_multiple = 7;   // OverlapF0Candidates' seven groups
+    cv.fixed_out = nullptr;
     return cv;
   }
 
@@ -1374,6 +1378,99 @@ int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* 
       check(launch_copy(x, n, y, s), "copy");
     }
     check(launch_remove_mean(bv, y, bins, s), "remove_mean");
+  });
+}
+
+int hv_contour_batch(const double* f0_candidates, const double* scores, const double* base,
+                     const int64_t* frame_offsets, int clips, int columns, int stride, int device, double* fixed,
+                     double* smoothed, unsigned flags, void* stream) {
+  return guarded([&] {
+    if (clips <= 0 || !frame_offsets) throw InvalidArgument("a batch needs at least one clip and its offsets");
+    if (!f0_candidates || !scores || !smoothed) throw InvalidArgument("null buffer");
+    if (stride < 1 || columns < 0 || columns > stride || columns > kRefineColumns)
+      throw InvalidArgument("require 0 <= columns <= stride, 1 <= stride and columns <= 1024");
+    if (frame_offsets[0] != 0) throw InvalidArgument("frame offsets must start at 0");
+    for (int c = 0; c < clips; ++c)
+      if (frame_offsets[c + 1] - frame_offsets[c] < 1 || frame_offsets[c + 1] - frame_offsets[c] >= (1 << 30))
+        throw InvalidArgument("every clip needs between 1 and 2^30 - 1 frames");
+    const int64_t F = frame_offsets[clips];
+    if (F >= (int64_t(1) << 31)) throw InvalidArgument("more than 2^31 frames");
+    const bool on_device = (flags & HV_DEVICE_POINTERS) != 0;
+    check_device(device);
+    WorkspaceCache::Lease lease(cache(), device);
+    Workspace& ws = lease.get();
+    ContextGuard guard(ws.ctx.get());
+    cudaStream_t st = ws.stream;
+    if (on_device && stream) st = static_cast<cudaStream_t>(stream);
+    else if (on_device && (flags & HV_NULL_IS_LEGACY_STREAM)) st = cudaStreamLegacy;
+    // Host tables: scratch offsets per clip, columns per clip.
+    std::vector<int64_t> scratch_off(clips + 1, 0);
+    for (int c = 0; c < clips; ++c)
+      scratch_off[c + 1] = scratch_off[c] + contour_scratch(frame_offsets[c + 1] - frame_offsets[c]);
+    std::vector<int> cols(clips, columns);
+    // Workspace buffer: [frame offsets | scratch offsets | columns | base |
+    // scratch | (host inputs: candidates, scores) | (host outputs: fixed,
+    // smoothed)].
+    const size_t o_f = 0, o_s = align_up(8 * size_t(clips + 1)), o_c = o_s + align_up(8 * size_t(clips + 1));
+    const size_t o_b = o_c + align_up(4 * size_t(clips));
+    const size_t o_sc = o_b + align_up(8 * size_t(F));
+    const size_t matrix = on_device ? 0 : align_up(8 * size_t(F) * size_t(stride));
+    const size_t o_in = o_sc + align_up(8 * size_t(scratch_off[clips]));
+    const size_t o_out = o_in + 2 * matrix;
+    const size_t need = o_out + (on_device ? 0 : 2 * align_up(8 * size_t(F)));
+    ws.contour_buf.reserve(need, ws.last, st, false, "cudaMalloc(contour)");
+    check(cudaStreamWaitEvent(st, ws.last, 0), "cudaStreamWaitEvent");
+    char* m = static_cast<char*>(ws.contour_buf.ptr);
+    int64_t* d_off = reinterpret_cast<int64_t*>(m + o_f);
+    int64_t* d_soff = reinterpret_cast<int64_t*>(m + o_s);
+    int* d_cols = reinterpret_cast<int*>(m + o_c);
+    double* d_base = reinterpret_cast<double*>(m + o_b);
+    const double* d_cand = f0_candidates;
+    const double* d_scores = scores;
+    double* d_fixed = fixed;
+    double* d_smoothed = smoothed;
+    check(cudaMemcpyAsync(d_off, frame_offsets, 8 * size_t(clips + 1), cudaMemcpyHostToDevice, st), "cudaMemcpy");
+    check(cudaMemcpyAsync(d_soff, scratch_off.data(), 8 * size_t(clips + 1), cudaMemcpyHostToDevice, st),
+          "cudaMemcpy");
+    check(cudaMemcpyAsync(d_cols, cols.data(), 4 * size_t(clips), cudaMemcpyHostToDevice, st), "cudaMemcpy");
+    if (!on_device) {
+      double* c_in = reinterpret_cast<double*>(m + o_in);
+      double* s_in = reinterpret_cast<double*>(m + o_in + matrix);
+      check(cudaMemcpyAsync(c_in, f0_candidates, 8 * size_t(F) * stride, cudaMemcpyHostToDevice, st), "cudaMemcpy");
+      check(cudaMemcpyAsync(s_in, scores, 8 * size_t(F) * stride, cudaMemcpyHostToDevice, st), "cudaMemcpy");
+      d_cand = c_in;
+      d_scores = s_in;
+      d_fixed = reinterpret_cast<double*>(m + o_out);
+      d_smoothed = reinterpret_cast<double*>(m + o_out + align_up(8 * size_t(F)));
+    }
+    if (base)
+      check(cudaMemcpyAsync(d_base, base, 8 * size_t(F), on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                            st),
+            "cudaMemcpy(base)");
+    else
+      check(launch_search_base(d_cand, d_scores, F, stride, d_off, clips, d_cols, d_base, st), "search_base");
+    ContourView cv{};
+    cv.batch.clips = clips;
+    cv.batch.capacity = stride;
+    cv.batch.frame_off = d_off;
+    cv.pruned = d_cand;
+    cv.pruned_scores = d_scores;
+    cv.best = d_base;
+    cv.count = d_cols;
+    cv.column_multiple = 1;
+    cv.scratch_off = d_soff;
+    cv.scratch = reinterpret_cast<double*>(m + o_sc);
+    cv.smoothed = d_smoothed;
+    cv.fixed_out = d_fixed;
+    cv.f0_out = nullptr;
+    check(launch_contour(cv, st), "contour");
+    if (!on_device) {
+      if (fixed)
+        check(cudaMemcpyAsync(fixed, d_fixed, 8 * size_t(F), cudaMemcpyDeviceToHost, st), "cudaMemcpy(fixed)");
+      check(cudaMemcpyAsync(smoothed, d_smoothed, 8 * size_t(F), cudaMemcpyDeviceToHost, st), "cudaMemcpy(smoothed)");
+    }
+    check(cudaEventRecord(ws.last, st), "cudaEventRecord");
+    if (!on_device) check(cudaStreamSynchronize(st), "contour");
   });
 }
 

@@ -64,8 +64,10 @@ struct ContourView {
   double* smoothed;             // [frames] 1 ms contour
   double period;                // frame_period in ms
   const int64_t* out_off;       // [clips + 1]
-  double* f0_out;
+  double* f0_out;               // resampled output; skipped when null
   double* t_out;
+  int column_multiple;          // candidate columns of clip c: column_multiple * count[c]
+  double* fixed_out;            // [frames] FixF0Contour's result, when not null
 };
 
 // The F0 gradient holds every discrete choice of the forward pass fixed.
@@ -194,5 +196,8 @@ cudaError_t launch_remove_mean_adjoint(const BatchView& v, double* grad_y, cudaS
 cudaError_t launch_decimate_adjoint(const DecimateView& v, const double* grad_y, double* u, double* states,
                                     int64_t segments, double* grad_x, cudaStream_t stream);
 cudaError_t launch_contour(const ContourView& v, cudaStream_t stream);
+cudaError_t launch_search_base(const double* cand, const double* scores, int64_t total_frames, int stride,
+                               const int64_t* frame_off, int clips, const int* columns, double* base,
+                               cudaStream_t stream);
 
 }  // namespace hv

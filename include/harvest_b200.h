@@ -192,6 +192,25 @@ HV_API int hv_harvest_stages(const double* x, int64_t n, int fs, double f0_floor
                              double* refined, double* scores, double* pruned,
                              double* pruned_scores, double* best, double* smoothed);
 
+/* Contour stage on caller-given candidates: FixF0Contour and
+ * SmoothF0Contour of WORLD (reference third_party/world/src/harvest.cpp:
+ * 693-1113; the reference's own host adapters are src/engine.cpp:55-214),
+ * run by the engine's contour kernel exactly as hv_harvest runs them after
+ * pruning. f0_candidates and scores are [F][stride] row-major (F =
+ * frame_offsets[clips]); clip c owns rows frame_offsets[c] ..
+ * frame_offsets[c + 1] - 1 (at least one row each) and its first `columns`
+ * columns are its candidates (WORLD's number_of_candidates). With base NULL
+ * the base contour is SearchF0Base's (highest score per frame, first on
+ * ties); otherwise FixStep1-4 start from base[F]. fixed[F] (may be NULL)
+ * receives FixF0Contour's result and smoothed[F] SmoothF0Contour's. Host
+ * pointers by default (the call waits); with HV_DEVICE_POINTERS every array
+ * is a device pointer and the work is enqueued on `stream` as for
+ * hv_harvest_batch. No counterpart of its own in the reference's ABI: it
+ * exposes the stage its tests/cpp/test_contour.cpp checks. */
+HV_API int hv_contour_batch(const double* f0_candidates, const double* scores, const double* base,
+                            const int64_t* frame_offsets, int clips, int columns, int stride, int device,
+                            double* fixed, double* smoothed, unsigned flags, void* stream);
+
 /* Allocation-free decimation: the decimation and DC-removal stage of
  * hv_harvest on one clip, for callers that cannot allocate device memory
  * at the point of the call: real-time audio callbacks that must not block

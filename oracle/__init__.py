@@ -59,6 +59,7 @@ class Checker:
         lib.oracle_stages.argtypes = [_D, ct.c_int, ct.c_int, ct.c_double, ct.c_double,
                                       _D, _D, _I, _D, _D, _D, _D, _D, _D, _D, _D]
         lib.oracle_fix_contour.argtypes = [_D, _D, ct.c_int, ct.c_int, ct.c_int, _D]
+        lib.oracle_fix_contour_base.argtypes = [_D, _D, _D, ct.c_int, ct.c_int, ct.c_int, _D]
         lib.oracle_smooth_contour.argtypes = [_D, ct.c_int, _D]
 
     def params(self, n, fs, f0_floor=71.0, f0_ceil=800.0):
@@ -95,14 +96,24 @@ class Checker:
         out["params"] = p
         return out
 
-    def fix_contour(self, cand, scores, columns=None):
+    def fix_contour(self, cand, scores, columns=None, base=None):
+        """FixF0Contour on [frames][stride] candidate and score matrices
+        (the first `columns` columns); with `base`, FixStep1-4 start from it
+        instead of SearchF0Base's contour."""
         cand = np.ascontiguousarray(cand, dtype=np.float64)
         scores = np.ascontiguousarray(scores, dtype=np.float64)
         frames, stride = cand.shape
+        if stride == 0:     # no candidate columns: keep the row pointers valid
+            cand, scores, stride = np.zeros((frames, 1)), np.zeros((frames, 1)), 1
+            columns = 0
         out = np.zeros(frames)
-        self.lib.oracle_fix_contour(_ptr(cand), _ptr(scores), frames,
-                                    stride if columns is None else int(columns), stride,
-                                    _ptr(out))
+        cols = stride if columns is None else int(columns)
+        if base is None:
+            self.lib.oracle_fix_contour(_ptr(cand), _ptr(scores), frames, cols, stride, _ptr(out))
+        else:
+            base = np.ascontiguousarray(base, dtype=np.float64)
+            self.lib.oracle_fix_contour_base(_ptr(base), _ptr(cand), _ptr(scores), frames, cols, stride,
+                                             _ptr(out))
         return out
 
     def smooth_contour(self, f0):

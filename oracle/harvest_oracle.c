@@ -748,6 +748,20 @@ void oracle_fix_contour(const double* cand, const double* scores, int frames, in
   fix_contour(cand, scores, frames, columns, stride, fixed_out);
 }
 
+/* FixStep1-4 of FixF0Contour (harvest.cpp:1027-1044) from a caller-given
+ * base contour in place of SearchF0Base's. */
+void oracle_fix_contour_base(const double* base, const double* cand, const double* scores, int frames,
+                             int columns, int stride, double* fixed_out) {
+  double* a = malloc(sizeof(double) * (size_t)(frames > 0 ? frames : 1));
+  double* b = malloc(sizeof(double) * (size_t)(frames > 0 ? frames : 1));
+  int* bl = malloc(sizeof(int) * (size_t)(frames + 1));
+  fix_step1(base, frames, 0.008, b);
+  fix_step2(b, frames, 6, a, bl);
+  fix_step3(a, frames, columns, stride, cand, 0.18, scores, b, bl);
+  fix_step4(b, frames, 9, fixed_out, bl);
+  free(a); free(b); free(bl);
+}
+
 void oracle_smooth_contour(const double* f0, int frames, double* out) {
   for (int i = 0; i < frames; ++i) out[i] = 0.0;
   smooth_contour(f0, frames, out);

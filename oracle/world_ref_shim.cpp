@@ -132,6 +132,22 @@ void oracle_fix_contour(const double* cand, const double* scores, int frames,
   FixF0Contour(c.data(), s.data(), frames, columns, fixed_out);
 }
 
+// FixStep1-4 of FixF0Contour (harvest.cpp:1027-1044) from a caller-given
+// base contour in place of SearchF0Base's.
+void oracle_fix_contour_base(const double* base, const double* cand, const double* scores, int frames,
+                             int columns, int stride, double* fixed_out) {
+  std::vector<const double*> c(frames), s(frames);
+  for (int i = 0; i < frames; ++i) {
+    c[i] = cand + size_t(i) * stride;
+    s[i] = scores + size_t(i) * stride;
+  }
+  std::vector<double> a(frames + 1), b(frames + 1);
+  FixStep1(base, frames, 0.008, b.data());
+  FixStep2(b.data(), frames, 6, a.data());
+  FixStep3(a.data(), frames, columns, c.data(), 0.18, s.data(), b.data());
+  FixStep4(b.data(), frames, 9, fixed_out);
+}
+
 // SmoothF0Contour alone (harvest.cpp:1079-1113).
 void oracle_smooth_contour(const double* f0, int frames, double* out) {
   for (int i = 0; i < frames; ++i) out[i] = 0.0;
