@@ -1,13 +1,15 @@
 // a14-a16: FixF0Contour, SmoothF0Contour and resampling to frame_period.
 //
-// One warp owns one clip; clips run in parallel. Within a clip the
-// data-parallel parts run across the 32 lanes: FixStep1, the boundary lists
-// (warp ballots over the voicing changes), FixStep2's pruning, the extension
-// of every voiced section, FixStep4's gap filling, the zero-lag smoothing of
-// every voiced section and the resampling. The steps whose result depends on
-// order stay in lane 0, exactly as the reference writes them: ExtendSub's
-// carried mean, MakeSortedOrder, and MergeF0's score sums. Given the same
-// candidates the warp reproduces WORLD bit for bit.
+// Three kernels per batch (contour_prepare, contour_extend, contour_finish,
+// below). The steps whose result depends on order run exactly as the
+// reference writes them, on one warp of the clip's block: ExtendSub's
+// carried mean, MakeSortedOrder, and MergeF0 with MergeF0Sub's score sums.
+// Everything else runs across many threads: FixStep1, the boundary lists
+// (warp ballots and a block scan), FixStep2's pruning, the two ExtendF0 runs
+// of every voiced section (a warp per section, many blocks per clip),
+// FixStep4's gap filling, the zero-lag smoothing of every voiced section and
+// the resampling. Given the same candidates the kernels reproduce WORLD bit
+// for bit, except for the smoothing of sections of 2048 frames or more.
 #include "hv_stages.cuh"
 
 namespace hv {
@@ -16,15 +18,52 @@ constexpr int kExtend = 101;      // ExtendF0 writes at most 101 frames per side
 constexpr int kTransient = 1024;  // per-lane buffer for a smoothing tail
 constexpr unsigned kAll = 0xffffffffu;
 
-// Doubles of scratch one clip of `frames` frames needs.
+constexpr int kContourThreads = 256;   // threads of a clip's block in contour_prepare / contour_finish
+constexpr int kContourWarps = kContourThreads / 32;
+constexpr int kZone = 100;             // body frames at each end whose SearchScore contour_extend records
+
+// Doubles of scratch one clip of `frames` frames needs (contour_adjoint
+// reuses the same space with a layout of its own).
 __host__ __device__ inline int64_t contour_scratch_doubles(int64_t frames) {
-  int64_t sections = (frames + 1) / 8 + 2;
-  // s1..s4, extension values, section records (8 ints each), boundary list
-  // (up to frames + 600 ints), per-lane smoothing tails, the shared tail for
-  // deferred sections, deferred-section list.
-  return 4 * frames + 2 * kExtend * sections + 4 * sections + (frames + 602) +
-         32 * kTransient + (frames + 600) + (frames + 602) / 2 + 64;
+  const int64_t cap = (frames + 1) / 8 + 2;   // voiced sections: runs of >= 7 frames
+  return 4 * frames + 4 * kExtend * cap + 2 * kZone * cap + 4 * cap + (frames + 602) +
+         int64_t(kContourThreads) * kTransient + kContourWarps * (frames + 600) + (frames + 602) / 2 +
+         (frames + 1) / 2 + 8 + 64;
 }
+
+// One clip's scratch as the three contour kernels use it.
+struct ContourScratch {
+  double *s1, *s2, *s3, *s4;   // FixStep1 .. FixStep4 contours (record_tape reads s3)
+  double* ext;                 // [cap][2][kExtend] forward and backward extension values
+  double* ext_sc;              // [cap][2][kExtend] their SearchScore values
+  double* zone_sc;             // [cap][2][kZone] SearchScore of the first and last kZone body frames
+  int* sec;                    // [cap][8] st, ed, extended st, extended ed, kept section, order,
+                               //          frames examined backward, forward
+  int* bl;                     // boundary lists, up to 2 (F + 602) ints
+  double* tails;               // kContourThreads x kTransient smoothing tails
+  double* shared_tail;         // kContourWarps x (F + 600)
+  int* deferred;               // sections whose tail needs the long buffer
+  int* own;                    // [F] section whose value merged frame j holds
+  int* meta;                   // [0] sections, [1] kept sections
+  int64_t cap;
+  __device__ ContourScratch(double* sc, int F) {
+    cap = (F + 1) / 8 + 2;
+    s1 = sc;
+    s2 = s1 + F;
+    s3 = s2 + F;
+    s4 = s3 + F;
+    ext = s4 + F;
+    ext_sc = ext + 2 * kExtend * cap;
+    zone_sc = ext_sc + 2 * kExtend * cap;
+    sec = reinterpret_cast<int*>(zone_sc + 2 * kZone * cap);
+    bl = sec + 8 * cap;
+    tails = reinterpret_cast<double*>(bl) + (F + 602);
+    shared_tail = tails + static_cast<int64_t>(kContourThreads) * kTransient;
+    deferred = reinterpret_cast<int*>(shared_tail + static_cast<int64_t>(kContourWarps) * (F + 600));
+    own = deferred + 2 * ((F + 602) / 2);
+    meta = own + 2 * ((F + 1) / 2);
+  }
+};
 
 // GetBoundaryList (harvest.cpp:727-743) over f(0..len), by all 32 lanes:
 // voicing changes are found 32 frames at a time with a ballot, and change
@@ -62,9 +101,50 @@ __device__ int warp_boundary_list(F f, int len, int* out) {
   return count;
 }
 
-// The contour stage runs one warp per clip and is bound by the latency of
-// dependent loads, so the sequential loops below load kChunk values ahead
-// into registers and then consume them in the reference's order.
+// GetBoundaryList by the whole block: each warp takes a contiguous part of
+// 1 .. len - 1 and counts its voicing changes with ballots; a scan over the
+// warps' counts places each warp's changes, which a second pass writes.
+// Returns the count on every thread. `red` is shared scratch of one int per
+// warp; the function starts and ends with a barrier.
+template <class F>
+__device__ int block_boundary_list(F f, int len, int* out, int* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int per = ((len - 1 + nw - 1) / nw + 31) / 32 * 32;
+  const int i_begin = 1 + warp * per, i_end = imin(len, i_begin + per);
+  auto change_at = [&](int i) -> bool {
+    const int now = (i == len - 1) ? 0 : (f(i) > 0 ? 1 : 0);
+    const int before = (i - 1 == 0) ? 0 : (f(i - 1) > 0 ? 1 : 0);
+    return now != before;
+  };
+  __syncthreads();
+  int count = 0;
+  for (int b = i_begin; b < i_end; b += 32) {
+    const int i = b + lane;
+    count += __popc(__ballot_sync(kAll, i < i_end && change_at(i)));
+  }
+  if (lane == 0) red[warp] = count;
+  __syncthreads();
+  int idx0 = 0, all = 0;
+  for (int w = 0; w < nw; ++w) {
+    if (w < warp) idx0 += red[w];
+    all += red[w];
+  }
+  for (int b = i_begin; b < i_end; b += 32) {
+    const int i = b + lane;
+    const bool ch = i < i_end && change_at(i);
+    const unsigned mask = __ballot_sync(kAll, ch);
+    if (ch) {
+      const int idx = idx0 + __popc(mask & ((1u << lane) - 1));
+      out[idx] = i - idx % 2;
+    }
+    idx0 += __popc(mask);
+  }
+  __syncthreads();
+  return all;
+}
+
+// The sequential loops below load kChunk values ahead into registers and
+// then consume them in the reference's order.
 constexpr int kChunk = 8;
 
 // SelectBestF0 (harvest.cpp:636-650) with the columns spread over the lanes
@@ -428,9 +508,137 @@ __device__ void smooth_section_warp(P padded, int st, int ed, int64_t len, doubl
   __syncwarp();
 }
 
-__global__ void __launch_bounds__(32) contour_clips(ContourView v) {
+// The contour stage runs as three kernels per batch. Each keeps WORLD's
+// order wherever a result depends on it; the work that does not is spread
+// over many threads:
+//   contour_prepare  (a block of 8 warps per clip): FixStep1, FixStep2 and
+//                    the voiced sections of the step-2 contour;
+//   contour_extend   (many blocks per clip, a warp per section): both
+//                    ExtendF0 runs of every section, recording with every
+//                    value it writes that value's SearchScore, and the
+//                    SearchScore of the first and last kZone body frames;
+//   contour_finish   (a block of 8 warps per clip): ExtendSub's carried
+//                    mean and MergeF0 in order on warp 0 (MergeF0Sub's score
+//                    sums read the recorded SearchScores), FixStep4,
+//                    SmoothF0Contour and the resampling.
+__global__ void __launch_bounds__(kContourThreads) contour_prepare(ContourView v) {
+  __shared__ int red[kContourWarps];
+  const int c = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
+  const BatchView& B = v.batch;
+  const int64_t row0 = B.frame_off[c];
+  const int F = static_cast<int>(B.frame_off[c + 1] - row0);
+  const ContourScratch S(v.scratch + v.scratch_off[c], F);
+  const double* base = v.best + row0;
+  // FixStep1 (harvest.cpp:710-722), allowed range 0.008.
+  for (int i = tid; i < F; i += nt) {
+    double out = 0.0;
+    const double b0 = base[i];
+    if (i >= 2 && b0 != 0.0) {
+      const double b1 = base[i - 1], b2 = base[i - 2];
+      const double ref = b1 * 2 - b2;
+      out = fabs((b0 - ref) / ref) > 0.008 && fabs((b0 - b1)) / b1 > 0.008 ? 0.0 : b0;
+    }
+    S.s1[i] = out;
+    S.s2[i] = out;
+  }
+  __syncthreads();
+  // FixStep2 (harvest.cpp:748-762): voiced runs shorter than 7 frames go.
+  int nb = block_boundary_list([&](int i) { return S.s1[i]; }, F, S.bl, red);
+  for (int i = tid; i < nb / 2; i += nt) {
+    if (S.bl[2 * i + 1] - S.bl[2 * i] >= 6) continue;
+    for (int j = S.bl[2 * i]; j <= S.bl[2 * i + 1]; ++j) S.s2[j] = 0.0;
+  }
+  __syncthreads();
+  for (int i = tid; i < F; i += nt) S.s3[i] = S.s2[i];
+  // The voiced sections of FixStep3 (harvest.cpp:968-975).
+  nb = block_boundary_list([&](int i) { return S.s2[i]; }, F, S.bl, red);
+  const int sections = imin(nb / 2, static_cast<int>(S.cap));
+  for (int i = tid; i < sections; i += nt) {
+    S.sec[8 * i + 0] = S.bl[2 * i];
+    S.sec[8 * i + 1] = S.bl[2 * i + 1];
+  }
+  if (tid == 0) S.meta[0] = sections;
+}
+
+// SearchScore (harvest.cpp:901-907) of `value` in one frame's row, by the
+// whole warp: each lane keeps the reference's running maximum over its
+// columns (a NaN score never replaces it), and the lanes' maxima combine
+// into the same value. Every lane returns it.
+__device__ __forceinline__ double warp_search_score(double value, const double* cand, const double* score,
+                                                    int columns) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int i = lane; i < columns; i += 32)
+    if (value == cand[i] && s < score[i]) s = score[i];
+  for (int o = 16; o; o >>= 1) {
+    const double t = __shfl_xor_sync(kAll, s, o);
+    if (s < t) s = t;
+  }
+  return s;
+}
+
+// One direction of ExtendF0 as extend_f0, also recording the SearchScore of
+// every value written (out_score[k]) from the same rows, and the number of
+// frames examined. Returns the last frame that took a value.
+__device__ int extend_f0_scored(const double* cand, const double* score, int64_t stride, int columns, int from,
+                                int dir, int steps, double cur, double* out, double* out_score, int& examined) {
+  const int lane = threadIdx.x & 31;
+  int reached = from, misses = 0;
+  examined = 0;
+  if (columns <= kRowSlots * 32) {
+    CandRow row, next, srow, snext;
+    if (steps > 0) {
+      row.load(cand + static_cast<int64_t>(from + dir) * stride, columns);
+      srow.load(score + static_cast<int64_t>(from + dir) * stride, columns);
+    }
+    for (int k = 0; k < steps; ++k) {
+      const int idx = from + dir * (k + 1);
+      if (k + 1 < steps) {
+        next.load(cand + static_cast<int64_t>(idx + dir) * stride, columns);
+        snext.load(score + static_cast<int64_t>(idx + dir) * stride, columns);
+      }
+      const double val = warp_select_best(cur, row, columns, 0.18);
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < kRowSlots; ++q)
+        if (lane + 32 * q < columns && val == row.c[q] && s < srow.c[q]) s = srow.c[q];
+      for (int o = 16; o; o >>= 1) {
+        const double t = __shfl_xor_sync(kAll, s, o);
+        if (s < t) s = t;
+      }
+      if (lane == 0) {
+        out[k] = val;
+        out_score[k] = s;
+      }
+      examined = k + 1;
+      if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
+      if (misses == 4) break;
+      row = next;
+      srow = snext;
+    }
+  } else {
+    for (int k = 0; k < steps; ++k) {
+      const int idx = from + dir * (k + 1);
+      const double* crow = cand + static_cast<int64_t>(idx) * stride;
+      const double val = warp_select_best(cur, crow, columns, 0.18);
+      const double s = warp_search_score(val, crow, score + static_cast<int64_t>(idx) * stride, columns);
+      if (lane == 0) {
+        out[k] = val;
+        out_score[k] = s;
+      }
+      examined = k + 1;
+      if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
+      if (misses == 4) break;
+    }
+  }
+  return reached;
+}
+
+__global__ void __launch_bounds__(kContourThreads) contour_extend(ContourView v) {
   const int c = blockIdx.x;
-  const int lane = threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.y * kContourWarps + (threadIdx.x >> 5);
+  const int nw = gridDim.y * kContourWarps;
   const BatchView& B = v.batch;
   const int64_t row0 = B.frame_off[c];
   const int F = static_cast<int>(B.frame_off[c + 1] - row0);
@@ -438,111 +646,136 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
   const int stride = B.capacity;
   const double* cand = v.pruned + row0 * stride;
   const double* score = v.pruned_scores + row0 * stride;
-  const double* base = v.best + row0;
-
-  double* sc = v.scratch + v.scratch_off[c];
-  const int64_t sections_cap = (F + 1) / 8 + 2;
-  double* s1 = sc;
-  double* s2 = s1 + F;
-  double* s3 = s2 + F;
-  double* s4 = s3 + F;
-  double* ext = s4 + F;                                              // [sections][2][kExtend]
-  int* sec = reinterpret_cast<int*>(ext + 2 * kExtend * sections_cap);  // 8 ints per section
-  int* bl = sec + 8 * sections_cap;                                  // F + 602 doubles of ints
-  double* tails = reinterpret_cast<double*>(bl) + (F + 602);         // 32 x kTransient
-  double* shared_tail = tails + 32 * kTransient;                     // F + 600
-  int* deferred = reinterpret_cast<int*>(shared_tail + F + 600);     // (F + 602) ints
-
-  // FixStep1 (harvest.cpp:710-722), allowed range 0.008; four groups of 32
-  // frames per iteration.
-  for (int i0 = lane; i0 < F; i0 += 128) {
-    double b0[4], b1[4], b2[4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = i0 + 32 * u;
-      b0[u] = i < F ? base[i] : 0.0;
-      b1[u] = i < F && i >= 2 ? base[i - 1] : 0.0;
-      b2[u] = i < F && i >= 2 ? base[i - 2] : 0.0;
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int i = i0 + 32 * u;
-      if (i >= F) break;
-      double out = 0.0;
-      if (i >= 2 && b0[u] != 0.0) {
-        double ref = b1[u] * 2 - b2[u];
-        out = fabs((b0[u] - ref) / ref) > 0.008 && fabs((b0[u] - b1[u])) / b1[u] > 0.008 ? 0.0 : b0[u];
-      }
-      s1[i] = out;
-      s2[i] = out;
-    }
-  }
-  __syncwarp();
-  // FixStep2 (harvest.cpp:748-762): voiced runs shorter than 7 frames go.
-  int nb = warp_boundary_list([&](int i) { return s1[i]; }, F, bl);
-  for (int i = lane; i < nb / 2; i += 32) {
-    if (bl[2 * i + 1] - bl[2 * i] >= 6) continue;
-    for (int j = bl[2 * i]; j <= bl[2 * i + 1]; ++j) s2[j] = 0.0;
-  }
-  __syncwarp();
-  for (int i = lane; i < F; i += 32) s3[i] = s2[i];
-  // FixStep3 (harvest.cpp:968-995): Extend/ExtendF0, one section at a time
-  // with the whole warp (each frame's SelectBestF0 across the lanes).
-  nb = warp_boundary_list([&](int i) { return s2[i]; }, F, bl);
-  const int sections = imin(nb / 2, static_cast<int>(sections_cap));
-  for (int i = 0; i < sections; ++i) {
-    const int st = bl[2 * i], ed = bl[2 * i + 1];
-    double* fwd = ext + (2 * i) * kExtend;
+  const ContourScratch S(v.scratch + v.scratch_off[c], F);
+  const int sections = S.meta[0];
+  for (int i = gw; i < sections; i += nw) {
+    const int st = S.sec[8 * i], ed = S.sec[8 * i + 1];
+    double* fwd = S.ext + (2 * i) * kExtend;
     double* bwd = fwd + kExtend;
+    double* fsc = S.ext_sc + (2 * i) * kExtend;
+    double* bsc = fsc + kExtend;
     for (int k = lane; k < kExtend; k += 32) fwd[k] = bwd[k] = 0.0;
     __syncwarp();
-    {  // ExtendF0 forward from the end (harvest.cpp:867-870)
-      const int reached = extend_f0(cand, stride, columns, ed, 1, imin(F - 2, ed + 100) - ed + 1, s2[ed], fwd);
-      if (lane == 0) sec[8 * i + 3] = reached;
+    int ef = 0, eb = 0;
+    // ExtendF0 forward from the end, then backward from the start (harvest.cpp:867-873).
+    const int rf = extend_f0_scored(cand, score, stride, columns, ed, 1, imin(F - 2, ed + 100) - ed + 1, S.s2[ed],
+                                    fwd, fsc, ef);
+    const int rb = extend_f0_scored(cand, score, stride, columns, st, -1, st - imax(1, st - 100) + 1, S.s2[st],
+                                    bwd, bsc, eb);
+    // SearchScore of the first and last kZone body frames (the only body
+    // frames whose scores MergeF0Sub can need without recomputing them).
+    double* head = S.zone_sc + (2 * i) * kZone;
+    double* tail = head + kZone;
+    for (int j = st; j <= imin(ed, st + kZone - 1); ++j) {
+      const double s = warp_search_score(S.s2[j], cand + static_cast<int64_t>(j) * stride,
+                                         score + static_cast<int64_t>(j) * stride, columns);
+      if (lane == 0) head[j - st] = s;
     }
-    {  // ExtendF0 backward from the start (harvest.cpp:871-873)
-      const int reached = extend_f0(cand, stride, columns, st, -1, st - imax(1, st - 100) + 1, s2[st], bwd);
-      if (lane == 0) sec[8 * i + 2] = reached;
+    for (int j = imax(st, ed - kZone + 1); j <= ed; ++j) {
+      const double s = warp_search_score(S.s2[j], cand + static_cast<int64_t>(j) * stride,
+                                         score + static_cast<int64_t>(j) * stride, columns);
+      if (lane == 0) tail[kZone - 1 - (ed - j)] = s;
     }
     if (lane == 0) {
-      sec[8 * i + 0] = st;
-      sec[8 * i + 1] = ed;
+      S.sec[8 * i + 2] = rb;
+      S.sec[8 * i + 3] = rf;
+      S.sec[8 * i + 6] = eb;
+      S.sec[8 * i + 7] = ef;
     }
   }
-  __syncwarp();
+}
+
+__global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v) {
+  __shared__ int red[kContourWarps];
+  __shared__ int deferred_count;
+  const int c = blockIdx.x;
+  const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+  const BatchView& B = v.batch;
+  const int64_t row0 = B.frame_off[c];
+  const int F = static_cast<int>(B.frame_off[c + 1] - row0);
+  const int columns = v.column_multiple * v.count[c];
+  const int stride = B.capacity;
+  const double* cand = v.pruned + row0 * stride;
+  const double* score = v.pruned_scores + row0 * stride;
+  const ContourScratch S(v.scratch + v.scratch_off[c], F);
+  const int sections = S.meta[0];
+  int* sec = S.sec;
+  int* bl = S.bl;
   // A section's extended row: its body from s2 plus the extension values.
   auto channel = [&](int i, int j) -> double {
     const int st = sec[8 * i], ed = sec[8 * i + 1];
-    if (j >= st && j <= ed) return s2[j];
-    if (j > ed && j - ed - 1 < kExtend) return ext[(2 * i) * kExtend + (j - ed - 1)];
-    if (j < st && st - 1 - j < kExtend) return ext[(2 * i + 1) * kExtend + (st - 1 - j)];
+    if (j >= st && j <= ed) return S.s2[j];
+    if (j > ed && j - ed - 1 < kExtend) return S.ext[(2 * i) * kExtend + (j - ed - 1)];
+    if (j < st && st - 1 - j < kExtend) return S.ext[(2 * i + 1) * kExtend + (st - 1 - j)];
     return 0.0;
   };
-  // ExtendSub (harvest.cpp:840-856): the running mean is never reset. The
-  // lanes load 32 channel values at a time and every lane adds them in
-  // order from shuffles, so all lanes hold the reference's sum. Kept
-  // sections keep their order; their section index goes to sec[8k + 4].
-  int kept = 0;
-  {
-    double mean = 0.0;
-    for (int i = 0; i < sections; ++i) {
-      const int st = sec[8 * i + 2], ed = sec[8 * i + 3];
-      for (int j0 = st; j0 < ed; j0 += 32) {
-        const double v = j0 + lane < ed ? channel(i, j0 + lane) : 0.0;
-        const int m = imin(32, ed - j0);
-        for (int k = 0; k < m; ++k) mean += __shfl_sync(kAll, v, k);
-      }
-      mean /= ed - st;
-      if (2200.0 / mean < ed - st) {
-        if (lane == 0) sec[8 * kept + 4] = i;
-        ++kept;
-      }
+  // SearchScore of section i's value at frame j: recorded by contour_extend
+  // for the frames its ExtendF0 runs examined and for the body's first and
+  // last kZone frames, computed here for any other frame.
+  auto score_of = [&](int i, int j, double value) -> double {
+    const int st = sec[8 * i], ed = sec[8 * i + 1];
+    if (j > ed) {
+      if (j - ed - 1 < sec[8 * i + 7]) return S.ext_sc[(2 * i) * kExtend + (j - ed - 1)];
+    } else if (j < st) {
+      if (st - 1 - j < sec[8 * i + 6]) return S.ext_sc[(2 * i + 1) * kExtend + (st - 1 - j)];
+    } else if (j - st < kZone) {
+      return S.zone_sc[(2 * i) * kZone + (j - st)];
+    } else if (ed - j < kZone) {
+      return S.zone_sc[(2 * i + 1) * kZone + (kZone - 1 - (ed - j))];
     }
+    return search_score(value, cand + static_cast<int64_t>(j) * stride, score + static_cast<int64_t>(j) * stride,
+                        columns);
+  };
+  // ExtendSub (harvest.cpp:840-856) on warp 0: the running mean is never
+  // reset. The walk goes over (section, 32 frames) chunks; each lane loads
+  // its value of the next chunk before the current one is summed, and every
+  // lane adds the current chunk's 32 values in order from shuffles, so all
+  // lanes hold the reference's sum. Kept sections keep their order; their
+  // section index goes to sec[8k + 4].
+  if (warp == 0) {
+    int kept = 0;
+    double mean = 0.0;
+    int i = 0, st = 0, ed = 0, j0 = 0;
+    double val = 0.0;
+    if (sections > 0) {
+      st = sec[2];
+      ed = sec[3];
+      j0 = st;
+      val = j0 + lane < ed ? channel(0, j0 + lane) : 0.0;
+    }
+    while (i < sections) {
+      int ni = i, nst = st, ned = ed, nj0 = j0 + 32;
+      if (nj0 >= ed) {
+        ni = i + 1;
+        if (ni < sections) {
+          nst = sec[8 * ni + 2];
+          ned = sec[8 * ni + 3];
+          nj0 = nst;
+        }
+      }
+      const double nval = ni < sections && nj0 + lane < ned ? channel(ni, nj0 + lane) : 0.0;
+      const int m = imin(32, ed - j0);
+      for (int k = 0; k < m; ++k) mean += __shfl_sync(kAll, val, k);
+      if (ni != i) {
+        mean /= ed - st;
+        if (2200.0 / mean < ed - st) {
+          if (lane == 0) sec[8 * kept + 4] = i;
+          ++kept;
+        }
+      }
+      i = ni;
+      st = nst;
+      ed = ned;
+      j0 = nj0;
+      val = nval;
+    }
+    if (lane == 0) S.meta[1] = kept;
   }
-  __syncwarp();
-  // MakeSortedOrder (harvest.cpp:883-896) in lane 0: extended bounds of the
-  // kept sections go to bl[2k], bl[2k+1] and the sort order to sec[8k + 5].
-  if (lane == 0) {
+  __syncthreads();
+  const int kept = S.meta[1];
+  // MakeSortedOrder (harvest.cpp:883-896) on thread 0: extended bounds of
+  // the kept sections go to bl[2k], bl[2k+1] and the sort order to sec[8k + 5].
+  if (tid == 0) {
     for (int k = 0; k < kept; ++k) {
       const int i = sec[8 * k + 4];
       bl[2 * k] = sec[8 * i + 2];
@@ -556,112 +789,124 @@ __global__ void __launch_bounds__(32) contour_clips(ContourView v) {
         else break;
       }
   }
-  __syncwarp();
+  __syncthreads();
   if (kept != 0) {
-    // MergeF0 (harvest.cpp:937-963): start from the first kept section, then
-    // lane 0 decides each merge (pair 0 of bl is the running extent) and
-    // the warp copies the chosen range.
+    // MergeF0 (harvest.cpp:937-963): start from the first kept section (every
+    // thread), then warp 0 merges in sorted order; own[j] names the section
+    // whose value merged frame j holds, for MergeF0Sub's score sums.
     const int first = sec[4];
-    for (int j = lane; j < F; j += 32) s3[j] = channel(first, j);
-    __syncwarp();
-    for (int i = 1; i < kept; ++i) {
-      const int o = sec[8 * i + 5];
-      const int ch = sec[8 * o + 4];
-      const int st2 = bl[2 * o], ed2 = bl[2 * o + 1];
-      const int st1 = bl[0], ed1 = bl[1];
-      int from = 0, to = -1;
-      if (st2 - ed1 > 0) {
-        from = st2;
-        to = ed2;
-      } else if (!(st1 <= st2 && ed1 >= ed2)) {   // MergeF0Sub (harvest.cpp:912-932)
-        // Scores of 32 frames at a time, one per lane, summed in order by
-        // every lane from shuffles.
-        double sc1 = 0.0, sc2 = 0.0;
-        for (int j0 = st2; j0 <= ed1; j0 += 32) {
-          const int j = j0 + lane;
-          double a = 0.0, b = 0.0;
-          if (j <= ed1) {
-            a = search_score(s3[j], cand + static_cast<int64_t>(j) * stride,
-                             score + static_cast<int64_t>(j) * stride, columns);
-            b = search_score(channel(ch, j), cand + static_cast<int64_t>(j) * stride,
-                             score + static_cast<int64_t>(j) * stride, columns);
-          }
-          const int m = imin(32, ed1 - j0 + 1);
-          for (int k = 0; k < m; ++k) {
-            sc1 += __shfl_sync(kAll, a, k);
-            sc2 += __shfl_sync(kAll, b, k);
-          }
-        }
-        from = sc1 > sc2 ? ed1 : st2;
-        to = ed2;
-      }
-      __syncwarp();
-      if (lane == 0 && to >= 0) {
-        if (st2 - ed1 > 0) bl[0] = st2;
-        bl[1] = ed2;
-      }
-      for (int j = from + lane; j <= to; j += 32) s3[j] = channel(ch, j);
-      __syncwarp();
+    for (int j = tid; j < F; j += nt) {
+      S.s3[j] = channel(first, j);
+      S.own[j] = first;
     }
+    __syncthreads();
+    if (warp == 0) {
+      for (int i = 1; i < kept; ++i) {
+        const int o = sec[8 * i + 5];
+        const int ch = sec[8 * o + 4];
+        const int st2 = bl[2 * o], ed2 = bl[2 * o + 1];
+        const int st1 = bl[0], ed1 = bl[1];
+        int from = 0, to = -1;
+        if (st2 - ed1 > 0) {
+          from = st2;
+          to = ed2;
+        } else if (!(st1 <= st2 && ed1 >= ed2)) {   // MergeF0Sub (harvest.cpp:912-932)
+          // Scores of 32 frames at a time, one per lane, summed in order by
+          // every lane from shuffles.
+          double sc1 = 0.0, sc2 = 0.0;
+          for (int j0 = st2; j0 <= ed1; j0 += 32) {
+            const int j = j0 + lane;
+            double a = 0.0, b = 0.0;
+            if (j <= ed1) {
+              a = score_of(S.own[j], j, S.s3[j]);
+              b = score_of(ch, j, channel(ch, j));
+            }
+            const int m = imin(32, ed1 - j0 + 1);
+            for (int k = 0; k < m; ++k) {
+              sc1 += __shfl_sync(kAll, a, k);
+              sc2 += __shfl_sync(kAll, b, k);
+            }
+          }
+          from = sc1 > sc2 ? ed1 : st2;
+          to = ed2;
+        }
+        __syncwarp();
+        if (lane == 0 && to >= 0) {
+          if (st2 - ed1 > 0) bl[0] = st2;
+          bl[1] = ed2;
+        }
+        for (int j = from + lane; j <= to; j += 32) {
+          S.s3[j] = channel(ch, j);
+          S.own[j] = ch;
+        }
+        __syncwarp();
+      }
+    }
+    __syncthreads();
   }
   // FixStep4 (harvest.cpp:1000-1022), threshold 9.
-  for (int i = lane; i < F; i += 32) s4[i] = s3[i];
-  __syncwarp();
-  nb = warp_boundary_list([&](int i) { return s3[i]; }, F, bl);
-  for (int i = lane; i < nb / 2 - 1; i += 32) {
+  for (int i = tid; i < F; i += nt) S.s4[i] = S.s3[i];
+  __syncthreads();
+  int nb = block_boundary_list([&](int i) { return S.s3[i]; }, F, bl, red);
+  for (int i = tid; i < nb / 2 - 1; i += nt) {
     const int distance = bl[2 * (i + 1)] - bl[2 * i + 1] - 1;
     if (distance >= 9) continue;
-    const double v0 = s3[bl[2 * i + 1]] + 1;
-    const double v1 = s3[bl[2 * (i + 1)]] - 1;
+    const double v0 = S.s3[bl[2 * i + 1]] + 1;
+    const double v1 = S.s3[bl[2 * (i + 1)]] - 1;
     const double slope = (v1 - v0) / (distance + 1.0);
     int cnt = 1;
-    for (int j = bl[2 * i + 1] + 1; j <= bl[2 * (i + 1)] - 1; ++j) s4[j] = v0 + slope * cnt++;
+    for (int j = bl[2 * i + 1] + 1; j <= bl[2 * (i + 1)] - 1; ++j) S.s4[j] = v0 + slope * cnt++;
   }
-  __syncwarp();
+  __syncthreads();
   if (v.fixed_out)
-    for (int i = lane; i < F; i += 32) v.fixed_out[row0 + i] = s4[i];
-  // SmoothF0Contour (harvest.cpp:1079-1113), one voiced section per lane.
+    for (int i = tid; i < F; i += nt) v.fixed_out[row0 + i] = S.s4[i];
+  // SmoothF0Contour (harvest.cpp:1079-1113): short sections one per
+  // thread, long ones one per warp.
   double* sm = v.smoothed + row0;
-  for (int i = lane; i < F; i += 32) sm[i] = 0.0;
-  __syncwarp();
+  for (int i = tid; i < F; i += nt) sm[i] = 0.0;
   const int lag = 300;
   const int64_t len = F + 2 * lag;
+  const double* s4 = S.s4;
   auto padded = [&](int j) -> double { return (j >= lag && j < lag + F) ? s4[j - lag] : 0.0; };
-  const int nbs = warp_boundary_list(padded, static_cast<int>(len), bl);
-  __shared__ int deferred_count;
-  if (lane == 0) deferred_count = 0;
-  __syncwarp();
-  for (int s = lane; s < nbs / 2; s += 32) {
+  const int nbs = block_boundary_list(padded, static_cast<int>(len), bl, red);
+  if (tid == 0) deferred_count = 0;
+  __syncthreads();
+  for (int s = tid; s < nbs / 2; s += nt) {
     if (bl[2 * s + 1] - bl[2 * s] + 1 >= kLongSection) continue;
-    if (!smooth_section(padded, bl[2 * s], bl[2 * s + 1], len, sm, tails + lane * kTransient, kTransient))
-      deferred[atomicAdd(&deferred_count, 1)] = s;
+    if (!smooth_section(padded, bl[2 * s], bl[2 * s + 1], len, sm, S.tails + tid * kTransient, kTransient))
+      S.deferred[atomicAdd(&deferred_count, 1)] = s;
   }
-  __syncwarp();
-  // Tails that had not settled within the lane buffer: redo with room for
-  // the whole padded length.
-  if (lane == 0)
+  __syncthreads();
+  // Tails that had not settled within the thread's buffer: redo with room
+  // for the whole padded length.
+  if (tid == 0)
     for (int k = 0; k < deferred_count; ++k) {
-      const int s = deferred[k];
-      smooth_section(padded, bl[2 * s], bl[2 * s + 1], len, sm, shared_tail, len);
+      const int s = S.deferred[k];
+      smooth_section(padded, bl[2 * s], bl[2 * s + 1], len, sm, S.shared_tail, len);
     }
-  __syncwarp();
-  // Long sections, one at a time with the whole warp.
+  __syncthreads();
+  // Long sections, one per warp.
+  int long_index = 0;
   for (int s = 0; s < nbs / 2; ++s)
-    if (bl[2 * s + 1] - bl[2 * s] + 1 >= kLongSection)
-      smooth_section_warp(padded, bl[2 * s], bl[2 * s + 1], len, sm, shared_tail, len);
+    if (bl[2 * s + 1] - bl[2 * s] + 1 >= kLongSection) {
+      if (long_index % kContourWarps == warp)
+        smooth_section_warp(padded, bl[2 * s], bl[2 * s + 1], len, sm, S.shared_tail + warp * (F + 600), len);
+      ++long_index;
+    }
+  __syncthreads();
   // Resampling (harvest.cpp:1246-1251); for frame_period 1 the same
   // expression reproduces the direct branch (harvest.cpp:1230-1235).
   if (!v.f0_out) return;
   const int64_t o0 = v.out_off[c];
   const int out_len = static_cast<int>(v.out_off[c + 1] - o0);
-  for (int i = lane; i < out_len; i += 32) {
+  for (int i = tid; i < out_len; i += nt) {
     const double t = i * v.period / 1000.0;
     v.t_out[o0 + i] = t;
     v.f0_out[o0 + i] = sm[imin(F - 1, matlab_round(t * 1000.0))];
   }
 }
 
-// Tape of the F0 gradient, written after contour_clips while its scratch is
+// Tape of the F0 gradient, written after contour_finish while its scratch is
 // live: per frame the step-3 value and the initial F0 of the candidate it
 // copies. Every nonzero step-3 value is a copy of a pruned candidate of its
 // own frame (FixStep1 keeps SearchF0Base's pick; ExtendF0 and MergeF0 copy
@@ -677,7 +922,7 @@ __global__ void record_tape(ContourView v, const double* __restrict__ cand, int6
   const int c = owner(B.frame_off, B.clips, gf);
   const int64_t row0 = B.frame_off[c];
   const int F = static_cast<int>(B.frame_off[c + 1] - row0);
-  const double fixed = v.scratch[v.scratch_off[c] + 2 * F + (gf - row0)];   // s3 of contour_clips
+  const double fixed = v.scratch[v.scratch_off[c] + 2 * F + (gf - row0)];   // s3 of the contour kernels
   double f0c = 0.0;
   if (fixed > 0.0) {
     const double* row = v.pruned + gf * B.capacity;
@@ -729,7 +974,7 @@ __global__ void __launch_bounds__(32) contour_adjoint(GradView v) {
     const double t = i * v.period / 1000.0;
     atomicAdd(g_sm + imin(F - 1, matlab_round(t * 1000.0)), v.grad_f0[o0 + i]);
   }
-  // FixStep4's fills, as contour_clips computes them.
+  // FixStep4's fills, as contour_finish computes them.
   int nb = warp_boundary_list([&](int i) { return s3[i]; }, F, bl);
   for (int i = lane; i < nb / 2 - 1; i += 32) {
     const int a = bl[2 * i + 1], b = bl[2 * (i + 1)];
@@ -800,7 +1045,9 @@ cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream) {
 }
 
 cudaError_t launch_contour(const ContourView& v, cudaStream_t stream) {
-  contour_clips<<<v.batch.clips, 32, 0, stream>>>(v);
+  contour_prepare<<<v.batch.clips, kContourThreads, 0, stream>>>(v);
+  contour_extend<<<dim3(v.batch.clips, v.extend_blocks > 1 ? v.extend_blocks : 1), kContourThreads, 0, stream>>>(v);
+  contour_finish<<<v.batch.clips, kContourThreads, 0, stream>>>(v);
   return cudaGetLastError();
 }
 

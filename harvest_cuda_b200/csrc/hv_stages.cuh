@@ -51,6 +51,12 @@ struct BankView {
   // dump[(band * total_blocks + block) * (valid + 2) + q], for the adjoint of
   // the per-band candidates.
   double* dump;
+  // FFT bank only: per CTA, per block of its current item and per thread
+  // run of the event scan, the four running event counts before the run
+  // (walk_index[(cta * walk_blocks + block) * 256 + thread]); the contour
+  // walk starts from them instead of searching the event lists.
+  int4* walk_index;
+  int64_t walk_blocks;       // most blocks of any clip
 };
 
 struct ContourView {
@@ -68,7 +74,15 @@ struct ContourView {
   double* t_out;
   int column_multiple;          // candidate columns of clip c: column_multiple * count[c]
   double* fixed_out;            // [frames] FixF0Contour's result, when not null
+  int extend_blocks;            // blocks per clip of the section-extension kernel
 };
+
+// Blocks per clip of the contour's section-extension kernel for a batch
+// whose longest clip has `max_frames` analysis frames.
+inline int contour_extend_blocks(int64_t max_frames) {
+  const int64_t b = (max_frames + 1023) / 1024;
+  return static_cast<int>(b < 1 ? 1 : (b > 32 ? 32 : b));
+}
 
 // The F0 gradient holds every discrete choice of the forward pass fixed.
 // Its tape has two doubles per 1 ms frame: the FixF0Contour step-3 value and,

@@ -76,6 +76,6 @@ def test_clock_sampler_without_nvml(monkeypatch):
 
 def test_kernels_per_step():
     # The finiteness flag, the decimation (6 kernels, or one copy when the
-    # rate needs no decimation), then 11 kernels of the fixed stages.
-    assert bench.kernels_per_step(2) == 18
-    assert bench.kernels_per_step(1) == 13
+    # rate needs no decimation), then 13 kernels of the fixed stages.
+    assert bench.kernels_per_step(2) == 20
+    assert bench.kernels_per_step(1) == 15
