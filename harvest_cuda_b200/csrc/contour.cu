@@ -10,6 +10,8 @@
 // FixStep4's gap filling, the zero-lag smoothing of every voiced section and
 // the resampling. Given the same candidates the kernels reproduce WORLD bit
 // for bit, except for the smoothing of sections of 2048 frames or more.
+#include <math_constants.h>
+
 #include "hv_stages.cuh"
 
 namespace hv {
@@ -28,7 +30,7 @@ __host__ __device__ inline int64_t contour_scratch_doubles(int64_t frames) {
   const int64_t cap = (frames + 1) / 8 + 2;   // voiced sections: runs of >= 7 frames
   return 4 * frames + 4 * kExtend * cap + 2 * kZone * cap + 4 * cap + (frames + 602) +
          int64_t(kContourThreads) * kTransient + kContourWarps * (frames + 600) + (frames + 602) / 2 +
-         (frames + 1) / 2 + 8 + 64;
+         frames + 8 + 64;
 }
 
 // One clip's scratch as the three contour kernels use it.
@@ -43,7 +45,7 @@ struct ContourScratch {
   double* tails;               // kContourThreads x kTransient smoothing tails
   double* shared_tail;         // kContourWarps x (F + 600)
   int* deferred;               // sections whose tail needs the long buffer
-  int* own;                    // [F] section whose value merged frame j holds
+  double* ms;                  // [F] recorded SearchScore of merged frame j's value, NaN if none
   int* meta;                   // [0] sections, [1] kept sections
   int64_t cap;
   __device__ ContourScratch(double* sc, int F) {
@@ -60,10 +62,47 @@ struct ContourScratch {
     tails = reinterpret_cast<double*>(bl) + (F + 602);
     shared_tail = tails + static_cast<int64_t>(kContourThreads) * kTransient;
     deferred = reinterpret_cast<int*>(shared_tail + static_cast<int64_t>(kContourWarps) * (F + 600));
-    own = deferred + 2 * ((F + 602) / 2);
-    meta = own + 2 * ((F + 1) / 2);
+    ms = reinterpret_cast<double*>(deferred + 2 * ((F + 602) / 2));
+    meta = reinterpret_cast<int*>(ms + F);
   }
 };
+
+// One voiced section's extended row and the SearchScores contour_extend
+// recorded for it, with its bounds held in registers.
+struct SectionRow {
+  int st, ed, examined_back, examined_fwd;
+  const double *fwd, *bwd, *fwd_sc, *bwd_sc, *head_sc, *tail_sc;
+  // The section's value at frame j: its body from the step-2 contour, the
+  // extension values beside it, 0 elsewhere.
+  __device__ __forceinline__ double value(const double* s2, int j) const {
+    if (j >= st && j <= ed) return s2[j];
+    if (j > ed && j - ed - 1 < kExtend) return fwd[j - ed - 1];
+    if (j < st && st - 1 - j < kExtend) return bwd[st - 1 - j];
+    return 0.0;
+  }
+  // The recorded SearchScore of value(j), or NaN if none was recorded.
+  __device__ __forceinline__ double recorded(int j) const {
+    if (j > ed) return j - ed - 1 < examined_fwd ? fwd_sc[j - ed - 1] : CUDART_NAN;
+    if (j < st) return st - 1 - j < examined_back ? bwd_sc[st - 1 - j] : CUDART_NAN;
+    if (j - st < kZone) return head_sc[j - st];
+    if (ed - j < kZone) return tail_sc[kZone - 1 - (ed - j)];
+    return CUDART_NAN;
+  }
+};
+__device__ __forceinline__ SectionRow section_row(const ContourScratch& S, int i) {
+  SectionRow r;
+  r.st = S.sec[8 * i];
+  r.ed = S.sec[8 * i + 1];
+  r.examined_back = S.sec[8 * i + 6];
+  r.examined_fwd = S.sec[8 * i + 7];
+  r.fwd = S.ext + (2 * i) * kExtend;
+  r.bwd = r.fwd + kExtend;
+  r.fwd_sc = S.ext_sc + (2 * i) * kExtend;
+  r.bwd_sc = r.fwd_sc + kExtend;
+  r.head_sc = S.zone_sc + (2 * i) * kZone;
+  r.tail_sc = r.head_sc + kZone;
+  return r;
+}
 
 // GetBoundaryList (harvest.cpp:727-743) over f(0..len), by all 32 lanes:
 // voicing changes are found 32 frames at a time with a ballot, and change
@@ -579,91 +618,166 @@ __device__ __forceinline__ double warp_search_score(double value, const double* 
 
 // One direction of ExtendF0 as extend_f0, also recording the SearchScore of
 // every value written (out_score[k]) from the same rows, and the number of
-// frames examined. Returns the last frame that took a value.
-__device__ int extend_f0_scored(const double* cand, const double* score, int64_t stride, int columns, int from,
-                                int dir, int steps, double cur, double* out, double* out_score, int& examined) {
+// frames examined. Rows of at most 32 NS columns are held in registers, D
+// frames ahead (the rows do not depend on the chain of picks), so a step
+// waits for no load. The pick and its score are the warp reductions of
+// warp_select_best and warp_search_score. Returns the last frame that took
+// a value.
+template <int NS, int D>
+__device__ int extend_f0_ahead(const double* cand, const double* score, int64_t stride, int columns, int from,
+                               int dir, int steps, double cur, double* out, double* out_score, int& examined) {
   const int lane = threadIdx.x & 31;
   int reached = from, misses = 0;
   examined = 0;
-  if (columns <= kRowSlots * 32) {
-    CandRow row, next, srow, snext;
-    if (steps > 0) {
-      row.load(cand + static_cast<int64_t>(from + dir) * stride, columns);
-      srow.load(score + static_cast<int64_t>(from + dir) * stride, columns);
-    }
-    for (int k = 0; k < steps; ++k) {
-      const int idx = from + dir * (k + 1);
-      if (k + 1 < steps) {
-        next.load(cand + static_cast<int64_t>(idx + dir) * stride, columns);
-        snext.load(score + static_cast<int64_t>(idx + dir) * stride, columns);
-      }
-      const double val = warp_select_best(cur, row, columns, 0.18);
-      double s = 0.0;
+  double rc[D][NS], rs[D][NS];
+  auto load = [&](double (&c)[NS], double (&sc)[NS], int k) {   // the row of step k
+    const bool live = k < steps;
+    const int64_t row = live ? static_cast<int64_t>(from + dir * (k + 1)) * stride : 0;
 #pragma unroll
-      for (int q = 0; q < kRowSlots; ++q)
-        if (lane + 32 * q < columns && val == row.c[q] && s < srow.c[q]) s = srow.c[q];
-      for (int o = 16; o; o >>= 1) {
-        const double t = __shfl_xor_sync(kAll, s, o);
-        if (s < t) s = t;
-      }
-      if (lane == 0) {
-        out[k] = val;
-        out_score[k] = s;
-      }
-      examined = k + 1;
-      if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
-      if (misses == 4) break;
-      row = next;
-      srow = snext;
+    for (int q = 0; q < NS; ++q) {
+      const bool ok = live && lane + 32 * q < columns;
+      c[q] = ok ? cand[row + lane + 32 * q] : 0.0;
+      sc[q] = ok ? score[row + lane + 32 * q] : 0.0;
     }
-  } else {
-    for (int k = 0; k < steps; ++k) {
-      const int idx = from + dir * (k + 1);
-      const double* crow = cand + static_cast<int64_t>(idx) * stride;
-      const double val = warp_select_best(cur, crow, columns, 0.18);
-      const double s = warp_search_score(val, crow, score + static_cast<int64_t>(idx) * stride, columns);
+  };
+#pragma unroll
+  for (int u = 0; u < D; ++u) load(rc[u], rs[u], u);
+  bool done = false;
+  for (int k0 = 0; k0 < steps && !done; k0 += D) {
+#pragma unroll
+    for (int u = 0; u < D; ++u) {
+      const int k = k0 + u;
+      if (k >= steps) {
+        done = true;
+        break;
+      }
+      // SelectBestF0 (harvest.cpp:636-650): smallest error within 0.18, the
+      // later column on ties.
+      double best_e = 0.18, val = 0.0;
+      int best_i = -1;
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        const int i = lane + 32 * q;
+        if (i >= columns) break;
+        const double e = fabs(cur - rc[u][q]) / cur;
+        if (e <= best_e) { best_e = e; best_i = i; val = rc[u][q]; }
+      }
+      for (int o = 16; o; o >>= 1) {
+        const double oe = __shfl_xor_sync(kAll, best_e, o), ov = __shfl_xor_sync(kAll, val, o);
+        const int oi = __shfl_xor_sync(kAll, best_i, o);
+        if (oi >= 0 && (best_i < 0 || oe < best_e || (oe == best_e && oi > best_i))) {
+          best_e = oe; best_i = oi; val = ov;
+        }
+      }
+      // SearchScore (harvest.cpp:901-907) of the pick in the same row.
+      double sc = 0.0;
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+        if (lane + 32 * q < columns && val == rc[u][q] && sc < rs[u][q]) sc = rs[u][q];
+      for (int o = 16; o; o >>= 1) {
+        const double t = __shfl_xor_sync(kAll, sc, o);
+        if (sc < t) sc = t;
+      }
+      load(rc[u], rs[u], k + D);
       if (lane == 0) {
         out[k] = val;
-        out_score[k] = s;
+        out_score[k] = sc;
       }
       examined = k + 1;
-      if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
-      if (misses == 4) break;
+      if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = from + dir * (k + 1); }
+      if (misses == 4) {
+        done = true;
+        break;
+      }
     }
   }
   return reached;
 }
 
-__global__ void __launch_bounds__(kContourThreads) contour_extend(ContourView v) {
-  const int c = blockIdx.x;
+// The same for rows wider than 256 columns, read from memory at each step.
+__device__ int extend_f0_wide(const double* cand, const double* score, int64_t stride, int columns, int from,
+                              int dir, int steps, double cur, double* out, double* out_score, int& examined) {
   const int lane = threadIdx.x & 31;
-  const int gw = blockIdx.y * kContourWarps + (threadIdx.x >> 5);
-  const int nw = gridDim.y * kContourWarps;
-  const BatchView& B = v.batch;
-  const int64_t row0 = B.frame_off[c];
-  const int F = static_cast<int>(B.frame_off[c + 1] - row0);
-  const int columns = v.column_multiple * v.count[c];
-  const int stride = B.capacity;
-  const double* cand = v.pruned + row0 * stride;
-  const double* score = v.pruned_scores + row0 * stride;
-  const ContourScratch S(v.scratch + v.scratch_off[c], F);
-  const int sections = S.meta[0];
-  for (int i = gw; i < sections; i += nw) {
-    const int st = S.sec[8 * i], ed = S.sec[8 * i + 1];
-    double* fwd = S.ext + (2 * i) * kExtend;
-    double* bwd = fwd + kExtend;
-    double* fsc = S.ext_sc + (2 * i) * kExtend;
-    double* bsc = fsc + kExtend;
-    for (int k = lane; k < kExtend; k += 32) fwd[k] = bwd[k] = 0.0;
-    __syncwarp();
-    int ef = 0, eb = 0;
-    // ExtendF0 forward from the end, then backward from the start (harvest.cpp:867-873).
-    const int rf = extend_f0_scored(cand, score, stride, columns, ed, 1, imin(F - 2, ed + 100) - ed + 1, S.s2[ed],
-                                    fwd, fsc, ef);
-    const int rb = extend_f0_scored(cand, score, stride, columns, st, -1, st - imax(1, st - 100) + 1, S.s2[st],
-                                    bwd, bsc, eb);
-    // SearchScore of the first and last kZone body frames (the only body
-    // frames whose scores MergeF0Sub can need without recomputing them).
+  int reached = from, misses = 0;
+  examined = 0;
+  for (int k = 0; k < steps; ++k) {
+    const int idx = from + dir * (k + 1);
+    const double* crow = cand + static_cast<int64_t>(idx) * stride;
+    const double val = warp_select_best(cur, crow, columns, 0.18);
+    const double s = warp_search_score(val, crow, score + static_cast<int64_t>(idx) * stride, columns);
+    if (lane == 0) {
+      out[k] = val;
+      out_score[k] = s;
+    }
+    examined = k + 1;
+    if (val == 0.0) ++misses; else { cur = val; misses = 0; reached = idx; }
+    if (misses == 4) break;
+  }
+  return reached;
+}
+
+// SearchScore of the step-2 value of frames j_lo .. j_hi (out[j - j_lo]),
+// by the warp, the rows of F frames loaded before any is reduced.
+template <int NS, int FR>
+__device__ void body_scores(const double* s2, const double* cand, const double* score, int64_t stride, int columns,
+                            int j_lo, int j_hi, double* out) {
+  const int lane = threadIdx.x & 31;
+  for (int j0 = j_lo; j0 <= j_hi; j0 += FR) {
+    double c[FR][NS], sc[FR][NS], v[FR];
+#pragma unroll
+    for (int f = 0; f < FR; ++f) {
+      const int j = j0 + f;
+      const bool live = j <= j_hi;
+      v[f] = live ? s2[j] : 0.0;
+      const int64_t row = live ? static_cast<int64_t>(j) * stride : 0;
+#pragma unroll
+      for (int q = 0; q < NS; ++q) {
+        const bool ok = live && lane + 32 * q < columns;
+        c[f][q] = ok ? cand[row + lane + 32 * q] : 0.0;
+        sc[f][q] = ok ? score[row + lane + 32 * q] : 0.0;
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < FR; ++f) {
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+        if (lane + 32 * q < columns && v[f] == c[f][q] && s < sc[f][q]) s = sc[f][q];
+      for (int o = 16; o; o >>= 1) {
+        const double t = __shfl_xor_sync(kAll, s, o);
+        if (s < t) s = t;
+      }
+      if (lane == 0 && j0 + f <= j_hi) out[j0 + f - j_lo] = s;
+    }
+  }
+}
+
+// Both ExtendF0 runs of section i and the SearchScores of its first and
+// last kZone body frames, by one warp.
+template <int NS, int D, int FR>
+__device__ void extend_section(const ContourScratch& S, int i, int F, const double* cand, const double* score,
+                               int stride, int columns) {
+  const int lane = threadIdx.x & 31;
+  const int st = S.sec[8 * i], ed = S.sec[8 * i + 1];
+  double* fwd = S.ext + (2 * i) * kExtend;
+  double* bwd = fwd + kExtend;
+  double* fsc = S.ext_sc + (2 * i) * kExtend;
+  double* bsc = fsc + kExtend;
+  for (int k = lane; k < kExtend; k += 32) fwd[k] = bwd[k] = 0.0;
+  __syncwarp();
+  int ef = 0, eb = 0, rf, rb;
+  // ExtendF0 forward from the end, then backward from the start (harvest.cpp:867-873).
+  const int steps_f = imin(F - 2, ed + 100) - ed + 1, steps_b = st - imax(1, st - 100) + 1;
+  if constexpr (NS > 0) {
+    rf = extend_f0_ahead<NS, D>(cand, score, stride, columns, ed, 1, steps_f, S.s2[ed], fwd, fsc, ef);
+    rb = extend_f0_ahead<NS, D>(cand, score, stride, columns, st, -1, steps_b, S.s2[st], bwd, bsc, eb);
+    body_scores<NS, FR>(S.s2, cand, score, stride, columns, st, imin(ed, st + kZone - 1), S.zone_sc + (2 * i) * kZone);
+    const int t_lo = imax(st, ed - kZone + 1);
+    body_scores<NS, FR>(S.s2, cand, score, stride, columns, t_lo, ed,
+                        S.zone_sc + (2 * i + 1) * kZone + (t_lo - (ed - kZone + 1)));
+  } else {
+    rf = extend_f0_wide(cand, score, stride, columns, ed, 1, steps_f, S.s2[ed], fwd, fsc, ef);
+    rb = extend_f0_wide(cand, score, stride, columns, st, -1, steps_b, S.s2[st], bwd, bsc, eb);
     double* head = S.zone_sc + (2 * i) * kZone;
     double* tail = head + kZone;
     for (int j = st; j <= imin(ed, st + kZone - 1); ++j) {
@@ -676,12 +790,32 @@ __global__ void __launch_bounds__(kContourThreads) contour_extend(ContourView v)
                                          score + static_cast<int64_t>(j) * stride, columns);
       if (lane == 0) tail[kZone - 1 - (ed - j)] = s;
     }
-    if (lane == 0) {
-      S.sec[8 * i + 2] = rb;
-      S.sec[8 * i + 3] = rf;
-      S.sec[8 * i + 6] = eb;
-      S.sec[8 * i + 7] = ef;
-    }
+  }
+  if (lane == 0) {
+    S.sec[8 * i + 2] = rb;
+    S.sec[8 * i + 3] = rf;
+    S.sec[8 * i + 6] = eb;
+    S.sec[8 * i + 7] = ef;
+  }
+}
+
+__global__ void __launch_bounds__(kContourThreads, 2) contour_extend(ContourView v) {
+  const int c = blockIdx.x;
+  const int gw = blockIdx.y * kContourWarps + (threadIdx.x >> 5);
+  const int nw = gridDim.y * kContourWarps;
+  const BatchView& B = v.batch;
+  const int64_t row0 = B.frame_off[c];
+  const int F = static_cast<int>(B.frame_off[c + 1] - row0);
+  const int columns = v.column_multiple * v.count[c];
+  const int stride = B.capacity;
+  const double* cand = v.pruned + row0 * stride;
+  const double* score = v.pruned_scores + row0 * stride;
+  const ContourScratch S(v.scratch + v.scratch_off[c], F);
+  const int sections = S.meta[0];
+  for (int i = gw; i < sections; i += nw) {
+    if (columns <= 128) extend_section<4, 4, 4>(S, i, F, cand, score, stride, columns);
+    else if (columns <= 256) extend_section<8, 2, 2>(S, i, F, cand, score, stride, columns);
+    else extend_section<0, 1, 1>(S, i, F, cand, score, stride, columns);
   }
 }
 
@@ -709,30 +843,63 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
     if (j < st && st - 1 - j < kExtend) return S.ext[(2 * i + 1) * kExtend + (st - 1 - j)];
     return 0.0;
   };
-  // SearchScore of section i's value at frame j: recorded by contour_extend
-  // for the frames its ExtendF0 runs examined and for the body's first and
-  // last kZone frames, computed here for any other frame.
-  auto score_of = [&](int i, int j, double value) -> double {
-    const int st = sec[8 * i], ed = sec[8 * i + 1];
-    if (j > ed) {
-      if (j - ed - 1 < sec[8 * i + 7]) return S.ext_sc[(2 * i) * kExtend + (j - ed - 1)];
-    } else if (j < st) {
-      if (st - 1 - j < sec[8 * i + 6]) return S.ext_sc[(2 * i + 1) * kExtend + (st - 1 - j)];
-    } else if (j - st < kZone) {
-      return S.zone_sc[(2 * i) * kZone + (j - st)];
-    } else if (ed - j < kZone) {
-      return S.zone_sc[(2 * i + 1) * kZone + (kZone - 1 - (ed - j))];
+  // ExtendSub (harvest.cpp:840-856): section i is kept when 2200 / mean_i
+  // < n_i, where mean_i = (mean_(i-1) + its n_i extended values, added in
+  // order) / n_i and the running mean is never reset. Only the decisions
+  // are used. Each warp first sums its sections' values in any order; with
+  // every value nonnegative, that sum and the reference's ordered one are
+  // both within (n_i + 1) u relative of the exact sum. Thread 0 then runs
+  // the recurrence on the warps' sums, carrying a bound on the relative
+  // error of its mean and of the reference's, and takes a decision only if
+  // 2200 / mean lies farther from n_i than that bound can move it. If any
+  // decision is that close, or any value is negative or not finite, warp 0
+  // repeats the reference's ordered sum exactly. Kept sections keep their
+  // order; their section index goes to sec[8k + 4].
+  double* sums = S.shared_tail;   // free until the smoothing
+  __shared__ int unsafe;
+  if (tid == 0) unsafe = 0;
+  __syncthreads();
+  for (int i = warp; i < sections; i += nt / 32) {
+    const int st = sec[8 * i + 2], ed = sec[8 * i + 3];
+    double part = 0.0;
+    bool bad = false;
+    for (int j = st + lane; j < ed; j += 32) {
+      const double x = channel(i, j);
+      bad |= !(x >= 0.0 && x <= 1.0e300);
+      part += x;
     }
-    return search_score(value, cand + static_cast<int64_t>(j) * stride, score + static_cast<int64_t>(j) * stride,
-                        columns);
-  };
-  // ExtendSub (harvest.cpp:840-856) on warp 0: the running mean is never
-  // reset. The walk goes over (section, 32 frames) chunks; each lane loads
-  // its value of the next chunk before the current one is summed, and every
-  // lane adds the current chunk's 32 values in order from shuffles, so all
-  // lanes hold the reference's sum. Kept sections keep their order; their
-  // section index goes to sec[8k + 4].
-  if (warp == 0) {
+    for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kAll, part, o);
+    if (__any_sync(kAll, bad) && lane == 0) unsafe = 1;
+    if (lane == 0) sums[i] = part;
+  }
+  __syncthreads();
+  if (tid == 0 && !unsafe) {
+    constexpr double u = 1.1102230246251565e-16;   // 2^-53
+    int kept = 0;
+    double mean = 0.0, err = 0.0;
+    for (int i = 0; i < sections && !unsafe; ++i) {
+      const int n = sec[8 * i + 3] - sec[8 * i + 2];
+      const double sum = mean + sums[i];
+      const double rho = sum > 0.0 ? mean / sum : 0.0;
+      err = err * rho + (n + 3) * u * 1.0001;
+      mean = sum / n;
+      if (sum == 0.0) continue;                     // exactly zero for both: never kept
+      const double ratio = 2200.0 / mean;
+      if (!(fabs(ratio - n) > ratio * (4.0 * err + 8.0 * u))) {
+        unsafe = 1;
+        break;
+      }
+      if (ratio < n) sec[8 * kept++ + 4] = i;
+    }
+    if (!unsafe) S.meta[1] = kept;
+  }
+  __syncthreads();
+  // The exact ordered sum, when a decision was too close to call: warp 0
+  // walks (section, 32 frames) chunks; each lane loads its value of the next
+  // chunk before the current one is summed, and every lane adds the current
+  // chunk's 32 values in order from shuffles, so all lanes hold the
+  // reference's sum.
+  if (unsafe && warp == 0) {
     int kept = 0;
     double mean = 0.0;
     int i = 0, st = 0, ed = 0, j0 = 0;
@@ -792,18 +959,24 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
   __syncthreads();
   if (kept != 0) {
     // MergeF0 (harvest.cpp:937-963): start from the first kept section (every
-    // thread), then warp 0 merges in sorted order; own[j] names the section
-    // whose value merged frame j holds, for MergeF0Sub's score sums.
-    const int first = sec[4];
+    // thread), then warp 0 merges in sorted order. ms[j] holds the
+    // SearchScore of merged frame j's value where contour_extend recorded it
+    // and NaN where it did not (a SearchScore is never NaN); MergeF0Sub's
+    // sums compute the missing ones.
+    const SectionRow first = section_row(S, sec[4]);
     for (int j = tid; j < F; j += nt) {
-      S.s3[j] = channel(first, j);
-      S.own[j] = first;
+      S.s3[j] = first.value(S.s2, j);
+      S.ms[j] = first.recorded(j);
     }
     __syncthreads();
     if (warp == 0) {
+      auto search = [&](double value, int j) {
+        return search_score(value, cand + static_cast<int64_t>(j) * stride,
+                            score + static_cast<int64_t>(j) * stride, columns);
+      };
       for (int i = 1; i < kept; ++i) {
         const int o = sec[8 * i + 5];
-        const int ch = sec[8 * o + 4];
+        const SectionRow row = section_row(S, sec[8 * o + 4]);
         const int st2 = bl[2 * o], ed2 = bl[2 * o + 1];
         const int st1 = bl[0], ed1 = bl[1];
         int from = 0, to = -1;
@@ -811,21 +984,29 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
           from = st2;
           to = ed2;
         } else if (!(st1 <= st2 && ed1 >= ed2)) {   // MergeF0Sub (harvest.cpp:912-932)
-          // Scores of 32 frames at a time, one per lane, summed in order by
-          // every lane from shuffles.
-          double sc1 = 0.0, sc2 = 0.0;
+          // Scores of 32 frames at a time, one per lane (the next 32 fetched
+          // before the current ones are added), summed in order by every
+          // lane from shuffles.
+          auto fetch = [&](int j, double& a, double& b) {
+            a = b = 0.0;
+            if (j > ed1) return;
+            a = S.ms[j];
+            if (a != a) a = search(S.s3[j], j);
+            b = row.recorded(j);
+            if (b != b) b = search(row.value(S.s2, j), j);
+          };
+          double sc1 = 0.0, sc2 = 0.0, a, b;
+          fetch(st2 + lane, a, b);
           for (int j0 = st2; j0 <= ed1; j0 += 32) {
-            const int j = j0 + lane;
-            double a = 0.0, b = 0.0;
-            if (j <= ed1) {
-              a = score_of(S.own[j], j, S.s3[j]);
-              b = score_of(ch, j, channel(ch, j));
-            }
+            double na, nb;
+            fetch(j0 + 32 + lane, na, nb);
             const int m = imin(32, ed1 - j0 + 1);
             for (int k = 0; k < m; ++k) {
               sc1 += __shfl_sync(kAll, a, k);
               sc2 += __shfl_sync(kAll, b, k);
             }
+            a = na;
+            b = nb;
           }
           from = sc1 > sc2 ? ed1 : st2;
           to = ed2;
@@ -836,8 +1017,8 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
           bl[1] = ed2;
         }
         for (int j = from + lane; j <= to; j += 32) {
-          S.s3[j] = channel(ch, j);
-          S.own[j] = ch;
+          S.s3[j] = row.value(S.s2, j);
+          S.ms[j] = row.recorded(j);
         }
         __syncwarp();
       }

@@ -190,7 +190,7 @@ struct Plan {
   bool use_fft = false;
   int fft_valid = 0;
   std::vector<int64_t> blk_off;
-  int64_t total_blocks = 0, max_blocks = 0;
+  int64_t total_blocks = 0;
   // Per-plan tables (offsets, work items, block offsets), uploaded to the
   // head of the arena by Workspace::prepare when another plan used it last.
   uint64_t id = 0;
@@ -199,8 +199,7 @@ struct Plan {
   size_t arena_bytes = 0;
   struct Layout {
     size_t meta, pcm, x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores,
-        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed, keys, leaders, item_off,
-        walk_index;
+        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed, keys, leaders, item_off;
   } at{};
   int bank_ctas = 0;
   // Device pointers, set by Workspace::prepare: into the arena's copy of
@@ -477,7 +476,6 @@ struct Workspace {
       for (int c = 0; c < B; ++c) {
         int64_t positions = p->y_off[c + 1] - p->y_off[c] - 1;   // event positions 0..y_len-2
         p->blk_off[c + 1] = p->blk_off[c] + (positions + p->fft_valid - 1) / p->fft_valid;
-        p->max_blocks = std::max(p->max_blocks, p->blk_off[c + 1] - p->blk_off[c]);
       }
       p->total_blocks = p->blk_off[B];
     }
@@ -565,7 +563,6 @@ struct Workspace {
     p->at.times = take(8 * p->out_off[B]);
     p->at.grad_y = take(8 * p->y_off[B]);
     p->at.grad_fixed = take(8 * F);
-    p->at.walk_index = take(sizeof(int4) * 256 * size_t(p->max_blocks) * size_t(p->bank_ctas));
     p->arena_bytes = off;
     return p;
   }
@@ -591,15 +588,13 @@ struct Workspace {
     return dv;
   }
 
-  BankView bank_view(const Plan& p) const {
+  static BankView bank_view(const Plan& p) {
     BankView kv{};
     kv.batch = batch_view(p);
     kv.centre = p.d_centre; kv.half = p.d_half; kv.tap_off = p.d_tap_off; kv.taps_rev = p.d_taps;
     kv.items = p.d_items; kv.item_count = static_cast<int>(p.items.size());
     kv.max_pad_taps = p.bank->max_pad_taps; kv.total_frames = p.frame_off[p.clips];
     kv.slot_capacity = p.slot_capacity;
-    kv.walk_index = p.use_fft ? ptr<int4>(p.at.walk_index) : nullptr;
-    kv.walk_blocks = p.max_blocks;
     return kv;
   }
 

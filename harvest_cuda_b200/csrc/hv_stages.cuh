@@ -51,12 +51,6 @@ struct BankView {
   // dump[(band * total_blocks + block) * (valid + 2) + q], for the adjoint of
   // the per-band candidates.
   double* dump;
-  // FFT bank only: per CTA, per block of its current item and per thread
-  // run of the event scan, the four running event counts before the run
-  // (walk_index[(cta * walk_blocks + block) * 256 + thread]); the contour
-  // walk starts from them instead of searching the event lists.
-  int4* walk_index;
-  int64_t walk_blocks;       // most blocks of any clip
 };
 
 struct ContourView {
