@@ -89,12 +89,13 @@ struct SectionRow {
     return CUDART_NAN;
   }
 };
-__device__ __forceinline__ SectionRow section_row(const ContourScratch& S, int i) {
+__device__ __forceinline__ SectionRow section_row(const ContourScratch& S, int i, int st, int ed, int examined_back,
+                                                  int examined_fwd) {
   SectionRow r;
-  r.st = S.sec[8 * i];
-  r.ed = S.sec[8 * i + 1];
-  r.examined_back = S.sec[8 * i + 6];
-  r.examined_fwd = S.sec[8 * i + 7];
+  r.st = st;
+  r.ed = ed;
+  r.examined_back = examined_back;
+  r.examined_fwd = examined_fwd;
   r.fwd = S.ext + (2 * i) * kExtend;
   r.bwd = r.fwd + kExtend;
   r.fwd_sc = S.ext_sc + (2 * i) * kExtend;
@@ -102,6 +103,9 @@ __device__ __forceinline__ SectionRow section_row(const ContourScratch& S, int i
   r.head_sc = S.zone_sc + (2 * i) * kZone;
   r.tail_sc = r.head_sc + kZone;
   return r;
+}
+__device__ __forceinline__ SectionRow section_row(const ContourScratch& S, int i) {
+  return section_row(S, i, S.sec[8 * i], S.sec[8 * i + 1], S.sec[8 * i + 6], S.sec[8 * i + 7]);
 }
 
 // GetBoundaryList (harvest.cpp:727-743) over f(0..len), by all 32 lanes:
@@ -855,41 +859,57 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
   // decision is that close, or any value is negative or not finite, warp 0
   // repeats the reference's ordered sum exactly. Kept sections keep their
   // order; their section index goes to sec[8k + 4].
+  // sums[2i], sums[2i + 1]: section i's sum and its length n_i.
   double* sums = S.shared_tail;   // free until the smoothing
   __shared__ int unsafe;
   if (tid == 0) unsafe = 0;
   __syncthreads();
   for (int i = warp; i < sections; i += nt / 32) {
+    const SectionRow r = section_row(S, i);
     const int st = sec[8 * i + 2], ed = sec[8 * i + 3];
     double part = 0.0;
     bool bad = false;
     for (int j = st + lane; j < ed; j += 32) {
-      const double x = channel(i, j);
+      const double x = r.value(S.s2, j);
       bad |= !(x >= 0.0 && x <= 1.0e300);
       part += x;
     }
     for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kAll, part, o);
     if (__any_sync(kAll, bad) && lane == 0) unsafe = 1;
-    if (lane == 0) sums[i] = part;
+    if (lane == 0) {
+      sums[2 * i] = part;
+      sums[2 * i + 1] = ed - st;
+    }
   }
   __syncthreads();
   if (tid == 0 && !unsafe) {
     constexpr double u = 1.1102230246251565e-16;   // 2^-53
     int kept = 0;
     double mean = 0.0, err = 0.0;
-    for (int i = 0; i < sections && !unsafe; ++i) {
-      const int n = sec[8 * i + 3] - sec[8 * i + 2];
-      const double sum = mean + sums[i];
-      const double rho = sum > 0.0 ? mean / sum : 0.0;
-      err = err * rho + (n + 3) * u * 1.0001;
-      mean = sum / n;
-      if (sum == 0.0) continue;                     // exactly zero for both: never kept
-      const double ratio = 2200.0 / mean;
-      if (!(fabs(ratio - n) > ratio * (4.0 * err + 8.0 * u))) {
-        unsafe = 1;
-        break;
+    // Eight sections' sums and lengths are loaded before they are used.
+    for (int i0 = 0; i0 < sections && !unsafe; i0 += 8) {
+      double sm[8], nn[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        sm[q] = i0 + q < sections ? sums[2 * (i0 + q)] : 0.0;
+        nn[q] = i0 + q < sections ? sums[2 * (i0 + q) + 1] : 1.0;
       }
-      if (ratio < n) sec[8 * kept++ + 4] = i;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        if (i0 + q >= sections || unsafe) break;
+        const double n = nn[q];
+        const double sum = mean + sm[q];
+        const double rho = sum > 0.0 ? mean / sum : 0.0;
+        err = err * rho + (n + 3.0) * u * 1.0001;
+        mean = sum / n;
+        if (sum == 0.0) continue;                     // exactly zero for both: never kept
+        const double ratio = 2200.0 / mean;
+        if (!(fabs(ratio - n) > ratio * (4.0 * err + 8.0 * u))) {
+          unsafe = 1;
+          break;
+        }
+        if (ratio < n) sec[8 * kept++ + 4] = i0 + q;
+      }
     }
     if (!unsafe) S.meta[1] = kept;
   }
@@ -940,15 +960,21 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
   }
   __syncthreads();
   const int kept = S.meta[1];
-  // MakeSortedOrder (harvest.cpp:883-896) on thread 0: extended bounds of
-  // the kept sections go to bl[2k], bl[2k+1] and the sort order to sec[8k + 5].
-  if (tid == 0) {
-    for (int k = 0; k < kept; ++k) {
-      const int i = sec[8 * k + 4];
-      bl[2 * k] = sec[8 * i + 2];
-      bl[2 * k + 1] = sec[8 * i + 3];
-      sec[8 * k + 5] = k;
-    }
+  // MakeSortedOrder (harvest.cpp:883-896): extended bounds of the kept
+  // sections go to bl[2k], bl[2k+1] (every thread) and the sort order to
+  // sec[8k + 5]. Kept sections come in order, and their extended starts
+  // nearly always are; only if some are not does thread 0 run the
+  // reference's insertion sort.
+  for (int k = tid; k < kept; k += nt) {
+    const int i = sec[8 * k + 4];
+    bl[2 * k] = sec[8 * i + 2];
+    bl[2 * k + 1] = sec[8 * i + 3];
+    sec[8 * k + 5] = k;
+  }
+  __syncthreads();
+  int inversions = 0;
+  for (int k = tid; k + 1 < kept; k += nt) inversions |= bl[2 * k] > bl[2 * (k + 1)];
+  if (__syncthreads_or(inversions) && tid == 0) {
     for (int i = 1; i < kept; ++i)
       for (int j = i - 1; j >= 0; --j) {
         const int oi = sec[8 * i + 5], oj = sec[8 * j + 5];
@@ -958,11 +984,39 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
   }
   __syncthreads();
   if (kept != 0) {
-    // MergeF0 (harvest.cpp:937-963): start from the first kept section (every
-    // thread), then warp 0 merges in sorted order. ms[j] holds the
+    // MergeF0 (harvest.cpp:937-963): start from the first kept section
+    // (every thread), then warp 0 merges in sorted order. ms[j] holds the
     // SearchScore of merged frame j's value where contour_extend recorded it
     // and NaN where it did not (a SearchScore is never NaN); MergeF0Sub's
     // sums compute the missing ones.
+    //
+    // A merged section's values are copied over [from, ed2]. MergeF0Sub's
+    // sums of later merges read frames within 100 frames before a later
+    // section's body (extended starts are at most 101 frames before a body,
+    // and the running extent ends at most 101 frames after an earlier body);
+    // bodies do not overlap, so a later merge reads or overwrites at most
+    // this section's last 100 body frames and its extension. That part is
+    // copied at once; the rest of the range (its body before them) is
+    // copied by every thread after the last merge.
+    //
+    // recs[i] for sorted position i: section, extended bounds (bl), and
+    // the body start and end, filled in parallel; the sequential loop loads
+    // the next merge's record before it works on the current one.
+    int* recs = reinterpret_cast<int*>(sums);     // 8 ints per kept section
+    int* lazy = recs + 8 * static_cast<int64_t>(kept);   // per merge: deferred copy [from, to], section
+    for (int i = tid; i < kept; i += nt) {
+      const int o = sec[8 * i + 5], ch = sec[8 * o + 4];
+      recs[8 * i + 0] = ch;
+      recs[8 * i + 1] = o;
+      recs[8 * i + 2] = bl[2 * o];
+      recs[8 * i + 3] = bl[2 * o + 1];
+      recs[8 * i + 4] = sec[8 * ch];
+      recs[8 * i + 5] = sec[8 * ch + 1];
+      recs[8 * i + 6] = sec[8 * ch + 6];
+      recs[8 * i + 7] = sec[8 * ch + 7];
+      lazy[4 * i + 0] = 0;
+      lazy[4 * i + 1] = -1;
+    }
     const SectionRow first = section_row(S, sec[4]);
     for (int j = tid; j < F; j += nt) {
       S.s3[j] = first.value(S.s2, j);
@@ -974,11 +1028,18 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
         return search_score(value, cand + static_cast<int64_t>(j) * stride,
                             score + static_cast<int64_t>(j) * stride, columns);
       };
+      int st1 = bl[0], ed1 = bl[1];   // the running extent (bl[0], bl[1] in the reference)
+      int next[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      if (kept > 1)
+        for (int q = 0; q < 8; ++q) next[q] = recs[8 + q];
       for (int i = 1; i < kept; ++i) {
-        const int o = sec[8 * i + 5];
-        const SectionRow row = section_row(S, sec[8 * o + 4]);
-        const int st2 = bl[2 * o], ed2 = bl[2 * o + 1];
-        const int st1 = bl[0], ed1 = bl[1];
+        const int ch = next[0], o = next[1];
+        // A section whose bounds are pair 0 reads the running extent, as the
+        // reference's boundary_list[order[i] * 2] does after earlier merges.
+        const int st2 = o == 0 ? st1 : next[2], ed2 = o == 0 ? ed1 : next[3];
+        const SectionRow row = section_row(S, ch, next[4], next[5], next[6], next[7]);
+        if (i + 1 < kept)
+          for (int q = 0; q < 8; ++q) next[q] = recs[8 * (i + 1) + q];
         int from = 0, to = -1;
         if (st2 - ed1 > 0) {
           from = st2;
@@ -1011,17 +1072,50 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
           from = sc1 > sc2 ? ed1 : st2;
           to = ed2;
         }
-        __syncwarp();
-        if (lane == 0 && to >= 0) {
-          if (st2 - ed1 > 0) bl[0] = st2;
-          bl[1] = ed2;
-        }
-        for (int j = from + lane; j <= to; j += 32) {
-          S.s3[j] = row.value(S.s2, j);
-          S.ms[j] = row.recorded(j);
+        if (to >= 0) {
+          if (st2 - ed1 > 0) st1 = st2;
+          ed1 = ed2;
+          // The part later merges may read or overwrite now (values loaded
+          // for the whole stretch before any is stored), the rest later.
+          const int now = imax(from, row.ed - 99);
+          if (lane == 0 && now > from) {
+            lazy[4 * i + 0] = from;
+            lazy[4 * i + 1] = now - 1;
+            lazy[4 * i + 2] = ch;
+          }
+          for (int j0 = now; j0 <= to; j0 += 128) {
+            double v[4], r[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int j = j0 + 32 * q + lane;
+              v[q] = j <= to ? row.value(S.s2, j) : 0.0;
+              r[q] = j <= to ? row.recorded(j) : 0.0;
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+              const int j = j0 + 32 * q + lane;
+              if (j <= to) {
+                S.s3[j] = v[q];
+                S.ms[j] = r[q];
+              }
+            }
+          }
         }
         __syncwarp();
       }
+      if (lane == 0) {
+        bl[0] = st1;
+        bl[1] = ed1;
+      }
+    }
+    __syncthreads();
+    // The deferred body copies, one merge per warp; no later merge read or
+    // wrote those frames.
+    for (int i = 1 + warp; i < kept; i += nt / 32) {
+      const int from = lazy[4 * i + 0], to = lazy[4 * i + 1];
+      if (to < from) continue;
+      const SectionRow row = section_row(S, lazy[4 * i + 2]);
+      for (int j = from + lane; j <= to; j += 32) S.s3[j] = row.value(S.s2, j);
     }
     __syncthreads();
   }

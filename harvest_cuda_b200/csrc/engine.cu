@@ -211,8 +211,10 @@ struct Plan {
   int2* d_items;
   int64_t* d_blk_off = nullptr;
   double* filters = nullptr;   // [bands][4097] filter amplitudes of the FFT bank
-  // Refinement launch shape, chosen by the autotuner on the plan's first run.
+  // Refinement launch shape and contour extension blocks per clip, chosen by
+  // the autotuner on the plan's first run (extend_blocks 0: the default).
   RefineShape refine_shape;
+  int extend_blocks = 0;
   bool tuned = false;
   // Captured launch sequence for this plan at a given arena base.
   cudaGraphExec_t graph = nullptr;
@@ -269,7 +271,11 @@ struct Workspace {
   std::map<Settings, std::shared_ptr<const BankTables>> banks;
   // Autotuned refinement shapes by (fs, f0_floor, f0_ceil, log2 of the
   // batch's total samples).
-  std::map<std::tuple<int, double, double, int>, RefineShape> tuned_shapes;
+  struct Tuning {
+    RefineShape refine;
+    int extend_blocks;
+  };
+  std::map<std::tuple<int, double, double, int, int>, Tuning> tuned_shapes;
   std::list<std::unique_ptr<Plan>> plans;  // most recent first
   std::map<Settings, std::unique_ptr<DeviceBank>> device_banks;
   uint64_t next_plan_id = 1;
@@ -617,7 +623,7 @@ struct Workspace {
     cv.fixed_out = nullptr;
     int64_t longest = 0;
     for (int c = 0; c < p.clips; ++c) longest = std::max(longest, p.frame_off[c + 1] - p.frame_off[c]);
-    cv.extend_blocks = contour_extend_blocks(longest);
+    cv.extend_blocks = p.extend_blocks > 0 ? p.extend_blocks : contour_extend_blocks(longest);
     return cv;
   }
 
@@ -778,20 +784,32 @@ struct Workspace {
       check(launch_copy(grad_y, p.x_off[B], grad_x, s), "copy");
   }
 
-  // Autotuner: picks the refinement launch shape for the
-  // plan's key the first time a plan with that key runs. It runs the
-  // pipeline once to produce the refinement's inputs, then times the
-  // refinement stage alone under every candidate shape (each launched twice,
-  // the second timed, so that lazy module loading is not timed) and keeps the
-  // fastest. All shapes give bit-identical results, so tuning never changes
-  // an output. HARVEST_B200_AUTOTUNE=0 skips it and uses the default shape.
+  // Autotuner: picks the refinement launch shape and the contour's section-
+  // extension blocks per clip for the plan's key the first time a plan with
+  // that key runs. The key is fs, the f0 range, and the length buckets
+  // (floor of log2) of the batch's samples and of its longest clip's frames.
+  // It runs the pipeline once to produce the stages' inputs, then times the
+  // refinement alone under every candidate shape and the contour under every
+  // candidate block count (each launched twice, the second timed, so that
+  // lazy module loading is not timed) and keeps the fastest. Every candidate
+  // gives bit-identical results, so tuning never changes an output.
+  // HARVEST_B200_AUTOTUNE=0 skips it and uses the defaults.
   void autotune(Plan& p, cudaStream_t s) {
     p.tuned = true;
-    int64_t total = p.x_off[p.clips];
-    int bucket = 0;
-    while ((int64_t(2) << bucket) <= total) ++bucket;
-    const auto key = std::make_tuple(p.s.fs, p.s.floor, p.s.ceil, bucket);
+    auto log2_bucket = [](int64_t v) {
+      int b = 0;
+      while ((int64_t(2) << b) <= v) ++b;
+      return b;
+    };
+    int64_t longest = 0;
+    for (int c = 0; c < p.clips; ++c) longest = std::max(longest, p.frame_off[c + 1] - p.frame_off[c]);
+    const auto key = std::make_tuple(p.s.fs, p.s.floor, p.s.ceil, log2_bucket(p.x_off[p.clips]), log2_bucket(longest));
     g_tuning[2] = 0;
+    // HARVEST_B200_CONTOUR_BLOCKS=n forces the contour's extension blocks.
+    if (const char* forced = std::getenv("HARVEST_B200_CONTOUR_BLOCKS")) {
+      const int e = std::atoi(forced);
+      if (e >= 1 && e <= 64) p.extend_blocks = e;
+    }
     // HARVEST_B200_REFINE_SHAPE=min_blocks,blocks_per_sm forces a shape.
     if (const char* forced = std::getenv("HARVEST_B200_REFINE_SHAPE")) {
       int a = 0, b = 0;
@@ -802,7 +820,8 @@ struct Workspace {
     }
     auto it = tuned_shapes.find(key);
     if (it != tuned_shapes.end()) {
-      p.refine_shape = it->second;
+      p.refine_shape = it->second.refine;
+      if (!p.extend_blocks) p.extend_blocks = it->second.extend_blocks;
       return;
     }
     const char* env = std::getenv("HARVEST_B200_AUTOTUNE");
@@ -839,8 +858,28 @@ struct Workspace {
         check(cudaEventElapsedTime(&ms, marks[0], marks[1]), "cudaEventElapsedTime");
         if (best_ms == 0.0f || ms < best_ms) { best_ms = ms; best = shape; }
       }
-    tuned_shapes[key] = best;
+    // The contour, with the refinement's own outputs (the same bits under
+    // every shape) still in place.
+    int best_blocks = p.extend_blocks;
+    if (!best_blocks) {
+      best_ms = 0.0f;
+      for (int blocks : {1, 2, 4, 8, 16, 32}) {
+        p.extend_blocks = blocks;
+        const ContourView cv = contour_view(p);
+        for (int rep = 0; rep < 2; ++rep) {
+          check(cudaEventRecord(marks[0], s), "cudaEventRecord");
+          check(launch_contour(cv, s), "contour");
+          check(cudaEventRecord(marks[1], s), "cudaEventRecord");
+        }
+        check(cudaEventSynchronize(marks[1]), "cudaEventSynchronize");
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, marks[0], marks[1]), "cudaEventElapsedTime");
+        if (best_ms == 0.0f || ms < best_ms) { best_ms = ms; best_blocks = blocks; }
+      }
+    }
+    tuned_shapes[key] = Tuning{best, best_blocks};
     p.refine_shape = best;
+    p.extend_blocks = best_blocks;
     g_tuning[2] = 1;
   }
 

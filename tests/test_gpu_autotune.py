@@ -1,6 +1,7 @@
-"""The autotuner of the refinement launch shape: every candidate shape gives
-bit-identical F0, tuning runs once per (fs, f0 range, length bucket) and is
-then reused, and HARVEST_B200_AUTOTUNE=0 falls back to the default shape."""
+"""The autotuner (the refinement's launch shape and the contour's section-
+extension blocks per clip): every candidate gives bit-identical F0, tuning
+runs once per (fs, f0 range, length buckets) and is then reused, and
+HARVEST_B200_AUTOTUNE=0 falls back to the default shape."""
 import ctypes as ct
 import os
 
@@ -72,3 +73,26 @@ def test_tuning_runs_once_per_key(gpu, clean_env):
     assert _last_tuning() == (4, 32, 0)
     for (f0, t), (wf, wt) in zip(first, off):
         assert np.array_equal(f0, wf) and np.array_equal(t, wt)
+
+
+def test_every_contour_block_count_gives_identical_f0(gpu, clean_env):
+    # Noisy 48 kHz clips with 1 ms frames have hundreds of voiced sections,
+    # which the contour's extension kernel spreads over its blocks.
+    saved = os.environ.get("HARVEST_B200_CONTOUR_BLOCKS")
+    try:
+        clips, _ = signals.ragged_batch(6, 48000, (2.0, 5.0), f0_range=(60.0, 600.0), snr_range=(0.0, 3.0),
+                                        seed=5)
+        want = None
+        for blocks in (1, 3, 8, 32):
+            hv.clear_cache()
+            os.environ["HARVEST_B200_CONTOUR_BLOCKS"] = str(blocks)
+            got = hv.harvest_many(clips, 48000, 71.0, 800.0, 1.0)
+            if want is None:
+                want = got
+            for (f0, t), (wf, wt) in zip(got, want):
+                assert np.array_equal(f0, wf) and np.array_equal(t, wt), blocks
+    finally:
+        if saved is None:
+            os.environ.pop("HARVEST_B200_CONTOUR_BLOCKS", None)
+        else:
+            os.environ["HARVEST_B200_CONTOUR_BLOCKS"] = saved

@@ -165,3 +165,27 @@ def test_contour_batch_rejects_bad_arguments(gpu):
         contour_batch(cand, cand, np.array([0, 10]), columns=5)   # more columns than the stride
     with pytest.raises(ValueError):
         contour_batch(cand, cand, np.array([0, 0, 10]))        # an empty clip
+
+
+def test_extend_sub_decisions_on_the_threshold(gpu, checker):
+    # ExtendSub keeps a section when 2200 / mean < its extended length n.
+    # A section of value 2200 / n over exactly n summed frames sits on the
+    # threshold, where the engine must fall back to the reference's ordered
+    # sum; sections after it then carry that exact mean. With no candidates,
+    # ExtendF0 stops at once: a base run over frames a..b becomes the
+    # section a+1..b (FixStep1 drops its first frame), n = b - a - 1.
+    trials = []
+    for n, others in ((10, 0), (11, 2), (20, 3), (8, 1), (40, 4)):
+        frames = 400
+        base = np.zeros(frames)
+        a = 20
+        base[a:a + n + 2] = 2200.0 / n
+        rng = np.random.default_rng(n)
+        start = a + n + 12
+        for _ in range(others):   # later sections, some on their own threshold
+            m = int(rng.integers(8, 40))
+            base[start:start + m + 2] = 2200.0 / m if rng.random() < 0.5 else float(rng.uniform(60, 600))
+            start += m + 12
+        trials.append((np.zeros((frames, 8)), np.zeros((frames, 8)), base))
+    results = run_batch(trials, use_base=True)
+    expect_equal(checker, trials, results, use_base=True)
