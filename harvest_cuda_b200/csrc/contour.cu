@@ -1045,9 +1045,16 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
           from = st2;
           to = ed2;
         } else if (!(st1 <= st2 && ed1 >= ed2)) {   // MergeF0Sub (harvest.cpp:912-932)
-          // Scores of 32 frames at a time, one per lane (the next 32 fetched
-          // before the current ones are added), summed in order by every
-          // lane from shuffles.
+          // The reference adds the n = ed1 - st2 + 1 scores of each side in
+          // frame order and copies from ed1 if the merged side's sum is the
+          // larger. Scores are nonnegative, so each ordered sum lies within
+          // (n - 1) u relative of the exact one, as does the warp's sum in
+          // any order: the lanes take 32 frames at a time (the next 32
+          // fetched first) and reduce them by a tree. The decision is taken
+          // from those sums when they differ by more than both errors can
+          // explain; when the two sides hold the same score at every frame
+          // the reference's sums are equal (not larger); otherwise (or if a
+          // sum is not finite) warp 0 repeats the ordered sums exactly.
           auto fetch = [&](int j, double& a, double& b) {
             a = b = 0.0;
             if (j > ed1) return;
@@ -1056,20 +1063,48 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
             b = row.recorded(j);
             if (b != b) b = search(row.value(S.s2, j), j);
           };
-          double sc1 = 0.0, sc2 = 0.0, a, b;
+          double t1 = 0.0, t2 = 0.0, a, b;
+          bool differ = false;
           fetch(st2 + lane, a, b);
           for (int j0 = st2; j0 <= ed1; j0 += 32) {
             double na, nb;
             fetch(j0 + 32 + lane, na, nb);
-            const int m = imin(32, ed1 - j0 + 1);
-            for (int k = 0; k < m; ++k) {
-              sc1 += __shfl_sync(kAll, a, k);
-              sc2 += __shfl_sync(kAll, b, k);
+            differ |= __any_sync(kAll, a != b);
+            double ra = a, rb = b;
+            for (int o = 16; o; o >>= 1) {
+              ra += __shfl_xor_sync(kAll, ra, o);
+              rb += __shfl_xor_sync(kAll, rb, o);
             }
+            t1 += ra;
+            t2 += rb;
             a = na;
             b = nb;
           }
-          from = sc1 > sc2 ? ed1 : st2;
+          bool larger;
+          const double n = ed1 - st2 + 1;
+          constexpr double u = 1.1102230246251565e-16;   // 2^-53
+          if (!differ) {
+            larger = false;
+          } else if (fabs(t1 - t2) > 4.0 * (n + 2.0) * u * (t1 + t2) && t1 + t2 <= 1.0e300) {
+            larger = t1 > t2;
+          } else {
+            // The reference's ordered sums: 32 frames a round from shuffles.
+            double sc1 = 0.0, sc2 = 0.0;
+            fetch(st2 + lane, a, b);
+            for (int j0 = st2; j0 <= ed1; j0 += 32) {
+              double na, nb;
+              fetch(j0 + 32 + lane, na, nb);
+              const int m = imin(32, ed1 - j0 + 1);
+              for (int k = 0; k < m; ++k) {
+                sc1 += __shfl_sync(kAll, a, k);
+                sc2 += __shfl_sync(kAll, b, k);
+              }
+              a = na;
+              b = nb;
+            }
+            larger = sc1 > sc2;
+          }
+          from = larger ? ed1 : st2;
           to = ed2;
         }
         if (to >= 0) {

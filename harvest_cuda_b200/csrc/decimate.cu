@@ -7,8 +7,9 @@
 // sample. The recurrence is sequential, so it is evaluated here as a blocked
 // state-passing scan:
 //   1. every segment of S samples computes its zero-state final state;
-//   2. one thread per clip chains the segment states with the exact 3x3
-//      transition matrix A^S (precomputed on the host);
+//   2. every segment's initial state is chained from the zero-state results
+//      of the segments before it with the exact 3x3 transition matrix
+//      T = A^S (precomputed on the host), one thread per segment;
 //   3. every segment reruns from its true initial state and writes outputs.
 // Each output therefore follows the reference recurrence sample by sample,
 // differing only by the rounding of the chained initial state.
@@ -68,45 +69,42 @@ __global__ void decimate_segment_states(DecimateView v, const double* __restrict
   states[3 * seg + 2] = s2;
 }
 
-// Chains zero-state segment results into true initial states, in place:
-// on return states[seg] holds the state entering the segment. One thread
-// per clip; the zero-state results of 8 segments are loaded before they are
-// chained, so the chain waits for memory once per 8 segments.
-__global__ void decimate_chain(DecimateView v, double* __restrict__ states) {
-  constexpr int kAhead = 8;
-  int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= v.clips) return;
-  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+// The initial state of every segment from the zero-state results z of the
+// segments before it: s_k = T s_(k-1) + z_(k-1) from s = 0 at the clip's
+// first segment, unrolled over the last kChainDepth segments (Horner's
+// order, the expressions of the sequential chain). The filters' poles lie
+// within radius 0.89 (ratio 12; 0.66 at ratio 2), so |T| <= 7e-13 and the
+// dropped term T^3 s_(k-3) is below 1e-36 of the state: the rounded result
+// is that of the full chain. One thread per segment.
+constexpr int kChainDepth = 3;
+__global__ void decimate_chain(DecimateView v, const double* __restrict__ z, int64_t segments,
+                               double* __restrict__ entry) {
+  const int64_t seg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  const int64_t first = v.seg_off[owner(v.seg_off, v.clips, seg)];
   const double* m = v.trans;
-  const int64_t end = v.seg_off[c + 1];
-  for (int64_t seg0 = v.seg_off[c]; seg0 < end; seg0 += kAhead) {
-    double z[3 * kAhead];
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
 #pragma unroll
-    for (int k = 0; k < kAhead; ++k)
-      if (seg0 + k < end) {
-        z[3 * k] = states[3 * (seg0 + k)];
-        z[3 * k + 1] = states[3 * (seg0 + k) + 1];
-        z[3 * k + 2] = states[3 * (seg0 + k) + 2];
-      }
-#pragma unroll
-    for (int k = 0; k < kAhead; ++k) {
-      if (seg0 + k >= end) break;
-      const int64_t seg = seg0 + k;
-      states[3 * seg] = s0; states[3 * seg + 1] = s1; states[3 * seg + 2] = s2;
-      double n0 = m[0] * s0 + m[1] * s1 + m[2] * s2 + z[3 * k];
-      double n1 = m[3] * s0 + m[4] * s1 + m[5] * s2 + z[3 * k + 1];
-      double n2 = m[6] * s0 + m[7] * s1 + m[8] * s2 + z[3 * k + 2];
-      s0 = n0; s1 = n1; s2 = n2;
-    }
+  for (int d = kChainDepth; d >= 1; --d) {
+    const int64_t k = seg - d;
+    if (k < first) continue;
+    const double n0 = m[0] * s0 + m[1] * s1 + m[2] * s2 + z[3 * k];
+    const double n1 = m[3] * s0 + m[4] * s1 + m[5] * s2 + z[3 * k + 1];
+    const double n2 = m[6] * s0 + m[7] * s1 + m[8] * s2 + z[3 * k + 2];
+    s0 = n0; s1 = n1; s2 = n2;
   }
+  entry[3 * seg] = s0;
+  entry[3 * seg + 1] = s1;
+  entry[3 * seg + 2] = s2;
 }
 
 // Pass 0 writes the forward output u; pass 1 writes the kept samples of the
 // backward output into y (before DC removal).
+constexpr int kDecimateThreads = 128;
+
 template <int kPass>
-__global__ void decimate_segment_run(DecimateView v, const double* __restrict__ x,
-                                     double* __restrict__ u, int64_t segments,
-                                     const double* __restrict__ states, double* __restrict__ y) {
+__global__ void decimate_segment_run(DecimateView v, const double* __restrict__ x, double* __restrict__ u,
+                                     int64_t segments, const double* __restrict__ states, double* __restrict__ y) {
   int64_t seg = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (seg >= segments) return;
   int c; int64_t begin, end;
@@ -341,17 +339,19 @@ __global__ void remove_mean_and_edge_bins(const BatchView v, double* __restrict_
 
 // Host-side launchers -------------------------------------------------------
 
+// `states` holds 6 doubles per segment: the zero-state results, then the
+// chained initial states.
 cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, double* states,
                             int64_t segments, double* y, cudaStream_t stream) {
-  const int threads = 128;
+  const int threads = kDecimateThreads;
   unsigned grid = static_cast<unsigned>((segments + threads - 1) / threads);
-  unsigned cgrid = static_cast<unsigned>((v.clips + threads - 1) / threads);
+  double* entry = states + 3 * segments;
   decimate_segment_states<0><<<grid, threads, 0, stream>>>(v, x, u, segments, states);
-  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
-  decimate_segment_run<0><<<grid, threads, 0, stream>>>(v, x, u, segments, states, y);
+  decimate_chain<<<grid, threads, 0, stream>>>(v, states, segments, entry);
+  decimate_segment_run<0><<<grid, threads, 0, stream>>>(v, x, u, segments, entry, y);
   decimate_segment_states<1><<<grid, threads, 0, stream>>>(v, x, u, segments, states);
-  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
-  decimate_segment_run<1><<<grid, threads, 0, stream>>>(v, x, u, segments, states, y);
+  decimate_chain<<<grid, threads, 0, stream>>>(v, states, segments, entry);
+  decimate_segment_run<1><<<grid, threads, 0, stream>>>(v, x, u, segments, entry, y);
   return cudaGetLastError();
 }
 
@@ -398,13 +398,14 @@ cudaError_t launch_decimate_adjoint(const DecimateView& v, const double* grad_y,
   const int threads = 128;
   unsigned grid = static_cast<unsigned>((segments + threads - 1) / threads);
   unsigned cgrid = static_cast<unsigned>((v.clips + threads - 1) / threads);
+  double* entry = states + 3 * segments;
   adjoint_segment_states<0><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states);
-  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
-  adjoint_segment_run<0><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states, grad_x);
+  decimate_chain<<<grid, threads, 0, stream>>>(v, states, segments, entry);
+  adjoint_segment_run<0><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, entry, grad_x);
   adjoint_segment_states<1><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states);
-  decimate_chain<<<cgrid, threads, 0, stream>>>(v, states);
-  adjoint_segment_run<1><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, states, grad_x);
-  adjoint_edges<<<cgrid, threads, 0, stream>>>(v, states, grad_x);
+  decimate_chain<<<grid, threads, 0, stream>>>(v, states, segments, entry);
+  adjoint_segment_run<1><<<grid, threads, 0, stream>>>(v, grad_y, u, segments, entry, grad_x);
+  adjoint_edges<<<cgrid, threads, 0, stream>>>(v, entry, grad_x);
   return cudaGetLastError();
 }
 

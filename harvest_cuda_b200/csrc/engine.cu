@@ -543,7 +543,7 @@ struct Workspace {
     p->at.pcm = take(2 * p->x_off[B]);
     p->at.x = take(8 * p->x_off[B]);
     p->at.u = take(8 * p->t_off[B]);
-    p->at.states = take(8 * 3 * p->total_seg);
+    p->at.states = take(8 * 6 * p->total_seg);   // zero-state results, chained initial states
     p->at.y = take(8 * p->y_off[B]);
     p->at.bins = take(8 * 3 * B);
     p->at.queue = take(16);
@@ -988,7 +988,7 @@ void validate_batch(const int64_t* offsets, int clips, int fs, double f0_floor, 
 // Scratch of hv_decimate_noalloc: a fixed array in the library's device
 // image, present on every GPU that loads the library for the life of the
 // process. It holds the forward low-pass pass (n + 2 lag + 18 doubles), the
-// segment states (3 per 256 samples) and a 16-word tail: the offset tables
+// segment states (6 per 256 samples) and a 16-word tail: the offset tables
 // (words 0-7), the FFT size (word 8) and the three edge bins (words 10-12)
 // that the DC-removal kernel writes.
 constexpr int max_decimation_lag() {
@@ -1002,7 +1002,7 @@ constexpr int64_t kNoAllocMaxSamples = int64_t(1) << 20;
 constexpr int64_t kNoAllocPadded = kNoAllocMaxSamples + 2 * kNoAllocMaxLag + 18;
 constexpr int64_t kNoAllocSegments = (kNoAllocPadded + kSegment - 1) / kSegment;
 constexpr int64_t kNoAllocMeta = 16;
-constexpr int64_t kNoAllocDoubles = kNoAllocPadded + 3 * kNoAllocSegments + kNoAllocMeta;
+constexpr int64_t kNoAllocDoubles = kNoAllocPadded + 6 * kNoAllocSegments + kNoAllocMeta;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 // Writes the one-clip offset tables into the scratch (no host copies).
@@ -1392,7 +1392,7 @@ int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* 
     const int64_t segments = ratio > 1 ? (padded + kSegment - 1) / kSegment : 0;
     double* u = dev.scratch;
     double* states = u + kNoAllocPadded;
-    int64_t* meta = reinterpret_cast<int64_t*>(states + 3 * kNoAllocSegments);
+    int64_t* meta = reinterpret_cast<int64_t*>(states + 6 * kNoAllocSegments);
     double* bins = reinterpret_cast<double*>(meta + 10);
     noalloc_tables<<<1, 1, 0, s>>>(meta, n, y_len, padded, segments, static_cast<int>(2 * y_len));
     check(cudaGetLastError(), "noalloc_tables");

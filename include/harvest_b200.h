@@ -226,7 +226,7 @@ HV_API int hv_contour_batch(const double* f0_candidates, const double* scores, c
  * hv_harvest_stages returns as y.
  *
  * The scratch is one fixed array in the library's device image (about
- * 8.5 MB, held on every GPU that loads the library until the process
+ * 8.6 MB, held on every GPU that loads the library until the process
  * exits), so n may not exceed 1048576 samples; longer input is rejected
  * with HV_INVALID_ARGUMENT. No cudaMalloc, cudaFree or other allocating
  * routine is called. The first call on a device looks up the array's
