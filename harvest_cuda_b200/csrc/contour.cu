@@ -823,6 +823,219 @@ __global__ void __launch_bounds__(kContourThreads, 2) contour_extend(ContourView
   }
 }
 
+// MergeF0Sub's comparison (harvest.cpp:919-927), by all 32 lanes: whether
+// the sum of fetch(j).a over j in [lo, hi] is larger than that of
+// fetch(j).b, each added in frame order as the reference does; fetch returns
+// 0, 0 for j > hi. Scores are nonnegative, so each ordered sum lies within
+// (n - 1) u relative of the exact one, as does the warp's sum in any order:
+// the lanes take 32 frames at a time (the next 32 fetched first) and reduce
+// them by a tree. The decision is taken from those sums when they differ by
+// more than both errors can explain; when the two sides hold the same score
+// at every frame the reference's sums are equal (not larger); otherwise (or
+// if a sum is not finite) the warp repeats the ordered sums exactly.
+template <class Fetch>
+__device__ bool merge_sum_larger(int lo, int hi, Fetch fetch) {
+  const int lane = threadIdx.x & 31;
+  double t1 = 0.0, t2 = 0.0, a, b;
+  bool differ = false;
+  fetch(lo + lane, a, b);
+  for (int j0 = lo; j0 <= hi; j0 += 32) {
+    double na, nb;
+    fetch(j0 + 32 + lane, na, nb);
+    differ |= __any_sync(kAll, a != b);
+    double ra = a, rb = b;
+    for (int o = 16; o; o >>= 1) {
+      ra += __shfl_xor_sync(kAll, ra, o);
+      rb += __shfl_xor_sync(kAll, rb, o);
+    }
+    t1 += ra;
+    t2 += rb;
+    a = na;
+    b = nb;
+  }
+  if (!differ) return false;
+  const double n = hi - lo + 1;
+  constexpr double u = 1.1102230246251565e-16;   // 2^-53
+  if (fabs(t1 - t2) > 4.0 * (n + 2.0) * u * (t1 + t2) && t1 + t2 <= 1.0e300) return t1 > t2;
+  // The reference's ordered sums: 32 frames a round from shuffles.
+  double sc1 = 0.0, sc2 = 0.0;
+  fetch(lo + lane, a, b);
+  for (int j0 = lo; j0 <= hi; j0 += 32) {
+    double na, nb;
+    fetch(j0 + 32 + lane, na, nb);
+    const int m = imin(32, hi - j0 + 1);
+    for (int k = 0; k < m; ++k) {
+      sc1 += __shfl_sync(kAll, a, k);
+      sc2 += __shfl_sync(kAll, b, k);
+    }
+    a = na;
+    b = nb;
+  }
+  return sc1 > sc2;
+}
+
+// MergeF0 (harvest.cpp:937-963) when the kept sections' extended starts come
+// sorted (MakeSortedOrder keeps the identity order), in parallel. With
+// position i's extended bounds st_i, ed_i, the running extent's end before
+// merge i is ed1_i = max_{k<i} ed_k: a merge that changes it (a gap, st_i >
+// ed1_i, or a MergeF0Sub that is not contained) sets it to ed_i > ed1_i, and
+// a contained one (ed_i <= ed1_i; the running start never exceeds st_i)
+// leaves it. So every merge's kind and sum range [st_i, ed1_i] are known up
+// front, and the merged contour over that range was last written by p_i,
+// the first position reaching the maximum (no merge between p_i and i
+// writes), wherever j >= from_{p_i}, the start of p_i's copy (position 0's
+// values cover every frame). The block therefore
+//   1. scans the maxima (warp 0),
+//   2. decides every MergeF0Sub as if p_i wrote its whole range (a warp per
+//      merge, the decision helper above),
+//   3. walks the merges in order on warp 0, taking each decision whose
+//      assumption from_{p_i} <= st_i holds and recomputing the others with
+//      every frame's last writer resolved through the p chain,
+//   4. copies each merge's values over the frames no later merge writes:
+//      [from_i, min(ed_i, min_{k>i} from_k - 1)] (later copies end later).
+// The merged contour is S.s3, filled beforehand with position 0's values.
+struct MergeScores {
+  const double *cand, *score;
+  int stride, columns;
+};
+__device__ __forceinline__ double section_score(const ContourScratch& S, const SectionRow& r, const MergeScores& q,
+                                                int j) {
+  const double rec = r.recorded(j);
+  if (rec == rec) return rec;
+  return search_score(r.value(S.s2, j), q.cand + static_cast<int64_t>(j) * q.stride,
+                      q.score + static_cast<int64_t>(j) * q.stride, q.columns);
+}
+
+__device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScores& q) {
+  constexpr int kGap = 1, kContained = 2, kSub = 3;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  const int* sec = S.sec;
+  int* bl = S.bl;
+  int* ed1 = reinterpret_cast<int*>(S.shared_tail);   // free until the smoothing
+  int* prev = ed1 + kept;
+  int* kind = prev + kept;
+  int* spec = kind + kept;
+  int* from = spec + kept;
+  int* until = from + kept;
+  auto row_at = [&](int k) { return section_row(S, sec[8 * k + 4]); };
+  // 1. Running maxima of the extended ends, first position on ties.
+  if (warp == 0) {
+    int cv = bl[1], ci = 0;
+    for (int i0 = 1; i0 < kept; i0 += 32) {
+      const int i = i0 + lane;
+      const int e = i < kept ? bl[2 * i + 1] : INT_MIN;
+      int v = e, x = i;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int ov = __shfl_up_sync(kAll, v, o), ox = __shfl_up_sync(kAll, x, o);
+        if (lane >= o && !(v > ov)) {
+          v = ov;
+          x = ox;
+        }
+      }
+      int pv = __shfl_up_sync(kAll, v, 1), px = __shfl_up_sync(kAll, x, 1);
+      if (lane == 0) pv = INT_MIN;
+      const int mv = pv > cv ? pv : cv, mx = pv > cv ? px : ci;
+      if (i < kept) {
+        ed1[i] = mv;
+        prev[i] = mx;
+        kind[i] = bl[2 * i] > mv ? kGap : (e <= mv ? kContained : kSub);
+      }
+      const int lv = __shfl_sync(kAll, v, 31), lx = __shfl_sync(kAll, x, 31);
+      if (lv > cv) {
+        cv = lv;
+        ci = lx;
+      }
+    }
+  }
+  __syncthreads();
+  // 2. Every MergeF0Sub decided against its p_i's values.
+  for (int i = 1 + warp; i < kept; i += warps) {
+    if (kind[i] != kSub) continue;
+    const SectionRow rp = row_at(prev[i]), ri = row_at(i);
+    const int lo = bl[2 * i], hi = ed1[i];
+    const bool larger = merge_sum_larger(lo, hi, [&](int j, double& a, double& b) {
+      a = b = 0.0;
+      if (j > hi) return;
+      a = section_score(S, rp, q, j);
+      b = section_score(S, ri, q, j);
+    });
+    if (lane == 0) spec[i] = larger;
+  }
+  __syncthreads();
+  // 3. The merges in order: copy starts, checked assumptions.
+  if (warp == 0) {
+    int st1 = bl[0];
+    for (int i0 = 1; i0 < kept; i0 += 32) {
+      const int i = i0 + lane;
+      int kd = 0, p = 0, sp = 0, st = 0, e1 = 0;
+      if (i < kept) {
+        kd = kind[i];
+        p = prev[i];
+        sp = kd == kSub ? spec[i] : 0;
+        st = bl[2 * i];
+        e1 = ed1[i];
+      }
+      const int m = imin(32, kept - i0);
+      for (int k = 0; k < m; ++k) {
+        const int kd_k = __shfl_sync(kAll, kd, k), p_k = __shfl_sync(kAll, p, k);
+        const int st_k = __shfl_sync(kAll, st, k), e1_k = __shfl_sync(kAll, e1, k);
+        bool larger = __shfl_sync(kAll, sp, k) != 0;
+        int fr = -1;
+        if (kd_k == kGap) {
+          fr = st_k;
+          st1 = st_k;
+        } else if (kd_k == kSub) {
+          if (p_k != 0 && from[p_k] > st_k) {
+            const SectionRow ri = row_at(i0 + k);
+            larger = merge_sum_larger(st_k, e1_k, [&](int j, double& a, double& b) {
+              a = b = 0.0;
+              if (j > e1_k) return;
+              int w = p_k;
+              while (w != 0 && j < from[w]) w = prev[w];
+              a = section_score(S, row_at(w), q, j);
+              b = section_score(S, ri, q, j);
+            });
+          }
+          fr = larger ? e1_k : st_k;
+        }
+        if (lane == 0) from[i0 + k] = fr;
+        __syncwarp();
+      }
+    }
+    // 4a. Where each copy ends: before the earliest later copy start.
+    int carry = INT_MAX;
+    for (int i1 = kept - 1; i1 >= 1; i1 -= 32) {
+      const int i = i1 - lane;
+      const int f = i >= 1 ? from[i] : -1;
+      int v = f >= 0 ? f : INT_MAX;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int ov = __shfl_up_sync(kAll, v, o);
+        if (lane >= o) v = imin(v, ov);
+      }
+      int later = __shfl_up_sync(kAll, v, 1);
+      if (lane == 0) later = INT_MAX;
+      later = imin(later, carry);
+      if (i >= 1 && f >= 0) until[i] = imin(bl[2 * i + 1], later == INT_MAX ? INT_MAX : later - 1);
+      carry = imin(carry, __shfl_sync(kAll, v, 31));
+    }
+    if (lane == 0) {
+      const int last = kept - 1;
+      bl[0] = st1;
+      bl[1] = kept > 1 ? imax(ed1[last], bl[2 * last + 1]) : bl[1];
+    }
+  }
+  __syncthreads();
+  // 4b. The copies, a warp per merge.
+  for (int i = 1 + warp; i < kept; i += warps) {
+    const int fr = from[i];
+    if (fr < 0) continue;
+    const int to = until[i];
+    const SectionRow r = row_at(i);
+    for (int j = fr + lane; j <= to; j += 32) S.s3[j] = r.value(S.s2, j);
+  }
+  __syncthreads();
+}
+
 __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v) {
   __shared__ int red[kContourWarps];
   __shared__ int deferred_count;
@@ -974,7 +1187,8 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
   __syncthreads();
   int inversions = 0;
   for (int k = tid; k + 1 < kept; k += nt) inversions |= bl[2 * k] > bl[2 * (k + 1)];
-  if (__syncthreads_or(inversions) && tid == 0) {
+  const bool sorted = !__syncthreads_or(inversions);
+  if (!sorted && tid == 0) {
     for (int i = 1; i < kept; ++i)
       for (int j = i - 1; j >= 0; --j) {
         const int oi = sec[8 * i + 5], oj = sec[8 * j + 5];
@@ -983,9 +1197,14 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
       }
   }
   __syncthreads();
-  if (kept != 0) {
-    // MergeF0 (harvest.cpp:937-963): start from the first kept section
-    // (every thread), then warp 0 merges in sorted order. ms[j] holds the
+  if (kept != 0 && sorted) {
+    const SectionRow first = section_row(S, sec[4]);
+    for (int j = tid; j < F; j += nt) S.s3[j] = first.value(S.s2, j);
+    merge_sorted(S, kept, MergeScores{cand, score, stride, columns});
+  } else if (kept != 0) {
+    // MergeF0 (harvest.cpp:937-963) in the reference's order, when
+    // MakeSortedOrder reorders the sections: start from the first kept
+    // section (every thread), then warp 0 merges in sorted order. ms[j] holds the
     // SearchScore of merged frame j's value where contour_extend recorded it
     // and NaN where it did not (a SearchScore is never NaN); MergeF0Sub's
     // sums compute the missing ones.
@@ -1045,65 +1264,14 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
           from = st2;
           to = ed2;
         } else if (!(st1 <= st2 && ed1 >= ed2)) {   // MergeF0Sub (harvest.cpp:912-932)
-          // The reference adds the n = ed1 - st2 + 1 scores of each side in
-          // frame order and copies from ed1 if the merged side's sum is the
-          // larger. Scores are nonnegative, so each ordered sum lies within
-          // (n - 1) u relative of the exact one, as does the warp's sum in
-          // any order: the lanes take 32 frames at a time (the next 32
-          // fetched first) and reduce them by a tree. The decision is taken
-          // from those sums when they differ by more than both errors can
-          // explain; when the two sides hold the same score at every frame
-          // the reference's sums are equal (not larger); otherwise (or if a
-          // sum is not finite) warp 0 repeats the ordered sums exactly.
-          auto fetch = [&](int j, double& a, double& b) {
+          const bool larger = merge_sum_larger(st2, ed1, [&](int j, double& a, double& b) {
             a = b = 0.0;
             if (j > ed1) return;
             a = S.ms[j];
             if (a != a) a = search(S.s3[j], j);
             b = row.recorded(j);
             if (b != b) b = search(row.value(S.s2, j), j);
-          };
-          double t1 = 0.0, t2 = 0.0, a, b;
-          bool differ = false;
-          fetch(st2 + lane, a, b);
-          for (int j0 = st2; j0 <= ed1; j0 += 32) {
-            double na, nb;
-            fetch(j0 + 32 + lane, na, nb);
-            differ |= __any_sync(kAll, a != b);
-            double ra = a, rb = b;
-            for (int o = 16; o; o >>= 1) {
-              ra += __shfl_xor_sync(kAll, ra, o);
-              rb += __shfl_xor_sync(kAll, rb, o);
-            }
-            t1 += ra;
-            t2 += rb;
-            a = na;
-            b = nb;
-          }
-          bool larger;
-          const double n = ed1 - st2 + 1;
-          constexpr double u = 1.1102230246251565e-16;   // 2^-53
-          if (!differ) {
-            larger = false;
-          } else if (fabs(t1 - t2) > 4.0 * (n + 2.0) * u * (t1 + t2) && t1 + t2 <= 1.0e300) {
-            larger = t1 > t2;
-          } else {
-            // The reference's ordered sums: 32 frames a round from shuffles.
-            double sc1 = 0.0, sc2 = 0.0;
-            fetch(st2 + lane, a, b);
-            for (int j0 = st2; j0 <= ed1; j0 += 32) {
-              double na, nb;
-              fetch(j0 + 32 + lane, na, nb);
-              const int m = imin(32, ed1 - j0 + 1);
-              for (int k = 0; k < m; ++k) {
-                sc1 += __shfl_sync(kAll, a, k);
-                sc2 += __shfl_sync(kAll, b, k);
-              }
-              a = na;
-              b = nb;
-            }
-            larger = sc1 > sc2;
-          }
+          });
           from = larger ? ed1 : st2;
           to = ed2;
         }
