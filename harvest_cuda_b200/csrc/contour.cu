@@ -835,30 +835,33 @@ __global__ void __launch_bounds__(kContourThreads, 2) contour_extend(ContourView
 // if a sum is not finite) the warp repeats the ordered sums exactly.
 template <class Fetch>
 __device__ bool merge_sum_larger(int lo, int hi, Fetch fetch) {
+  constexpr int kRounds = 8;   // rounds of 32 frames loaded before any is added
   const int lane = threadIdx.x & 31;
-  double t1 = 0.0, t2 = 0.0, a, b;
+  double t1 = 0.0, t2 = 0.0;
   bool differ = false;
-  fetch(lo + lane, a, b);
-  for (int j0 = lo; j0 <= hi; j0 += 32) {
-    double na, nb;
-    fetch(j0 + 32 + lane, na, nb);
-    differ |= __any_sync(kAll, a != b);
-    double ra = a, rb = b;
-    for (int o = 16; o; o >>= 1) {
-      ra += __shfl_xor_sync(kAll, ra, o);
-      rb += __shfl_xor_sync(kAll, rb, o);
+  for (int c0 = lo; c0 <= hi; c0 += 32 * kRounds) {
+    double a[kRounds], b[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) fetch(c0 + 32 * r + lane, a[r], b[r]);
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      if (c0 + 32 * r > hi) break;
+      differ |= __any_sync(kAll, a[r] != b[r]);
+      double ra = a[r], rb = b[r];
+      for (int o = 16; o; o >>= 1) {
+        ra += __shfl_xor_sync(kAll, ra, o);
+        rb += __shfl_xor_sync(kAll, rb, o);
+      }
+      t1 += ra;
+      t2 += rb;
     }
-    t1 += ra;
-    t2 += rb;
-    a = na;
-    b = nb;
   }
   if (!differ) return false;
   const double n = hi - lo + 1;
   constexpr double u = 1.1102230246251565e-16;   // 2^-53
   if (fabs(t1 - t2) > 4.0 * (n + 2.0) * u * (t1 + t2) && t1 + t2 <= 1.0e300) return t1 > t2;
   // The reference's ordered sums: 32 frames a round from shuffles.
-  double sc1 = 0.0, sc2 = 0.0;
+  double sc1 = 0.0, sc2 = 0.0, a, b;
   fetch(lo + lane, a, b);
   for (int j0 = lo; j0 <= hi; j0 += 32) {
     double na, nb;
@@ -874,23 +877,32 @@ __device__ bool merge_sum_larger(int lo, int hi, Fetch fetch) {
   return sc1 > sc2;
 }
 
-// MergeF0 (harvest.cpp:937-963) when the kept sections' extended starts come
-// sorted (MakeSortedOrder keeps the identity order), in parallel. With
+// MergeF0 (harvest.cpp:937-963) in parallel, for a sort order (sec[8i + 5],
+// from MakeSortedOrder) that keeps kept section 0 first: the reference reads
+// position i's bounds from boundary pair order[i], which aliases the running
+// extent (pair 0) only for section 0, and starts the merged contour from
+// section 0. Position i stands for kept section order[i]. With
 // position i's extended bounds st_i, ed_i, the running extent's end before
 // merge i is ed1_i = max_{k<i} ed_k: a merge that changes it (a gap, st_i >
 // ed1_i, or a MergeF0Sub that is not contained) sets it to ed_i > ed1_i, and
 // a contained one (ed_i <= ed1_i; the running start never exceeds st_i)
 // leaves it. So every merge's kind and sum range [st_i, ed1_i] are known up
-// front, and the merged contour over that range was last written by p_i,
-// the first position reaching the maximum (no merge between p_i and i
-// writes), wherever j >= from_{p_i}, the start of p_i's copy (position 0's
-// values cover every frame). The block therefore
-//   1. scans the maxima (warp 0),
-//   2. decides every MergeF0Sub as if p_i wrote its whole range (a warp per
-//      merge, the decision helper above),
-//   3. walks the merges in order on warp 0, taking each decision whose
-//      assumption from_{p_i} <= st_i holds and recomputing the others with
-//      every frame's last writer resolved through the p chain,
+// front. The merged contour over that range was last written by p_i, the
+// first position reaching the maximum (no merge between p_i and i writes),
+// from the start of p_i's copy on; before that by what p_i's own merge saw,
+// p_(p_i) from its copy start on, and so on down to position 0, whose values
+// cover every frame. A MergeF0Sub decision (copy from ed1_i if the merged
+// side's score sum is larger, else from st_i) is thus a function of the copy
+// starts along its p chain, and the copy starts solve a triangular system.
+// The block
+//   1. scans the maxima (warp 0);
+//   2. runs up to kIterations parallel rounds: every MergeF0Sub is decided
+//      by a warp from the current copy starts, and decided again only when
+//      a copy start on its chain changed since it was last decided. A round
+//      that changes no copy start means every decision used the final
+//      starts of its chain, i.e. the sequential solution;
+//   3. otherwise walks the merges in order on warp 0 and decides again
+//      every decision whose chain changed since it was taken;
 //   4. copies each merge's values over the frames no later merge writes:
 //      [from_i, min(ed_i, min_{k>i} from_k - 1)] (later copies end later).
 // The merged contour is S.s3, filled beforehand with position 0's values.
@@ -906,24 +918,80 @@ __device__ __forceinline__ double section_score(const ContourScratch& S, const S
                       q.score + static_cast<int64_t>(j) * q.stride, q.columns);
 }
 
+// The MergeF0Sub decision of position i (by all 32 lanes) from the copy
+// starts in `from`: whether the merged side's sum over [st, e1] is larger.
+// Unless `force`, it is only recomputed (`fresh`) if a copy start on the
+// chain was changed at or after iteration `since` (stamp), i.e. possibly
+// after the decision was last taken; otherwise it returns false. The chain's
+// last writers are held as up to kChain segments; a longer chain resolves
+// each frame's writer on its own.
+__device__ __forceinline__ bool merge_decision(const ContourScratch& S, const MergeScores& q, const int* from,
+                                               const int* prev, const int* stamp, const int* pch, int i, int st,
+                                               int e1, bool force, int since, bool& fresh) {
+  constexpr int kChain = 4;
+  int seg_lo[kChain], seg_ch[kChain], n = 0, w = prev[i];
+  fresh = force;
+  for (;;) {
+    const int fw = w == 0 ? INT_MIN : from[w];
+    if (w != 0 && stamp[w] >= since) fresh = true;
+    if (n < kChain) {
+      seg_lo[n] = fw;
+      seg_ch[n] = pch[w];
+    }
+    ++n;
+    if (w == 0 || fw <= st) break;
+    w = prev[w];
+  }
+  if (!fresh) return false;
+  const SectionRow ri = section_row(S, pch[i]);
+  return merge_sum_larger(st, e1, [&](int j, double& a, double& b) {
+    a = b = 0.0;
+    if (j > e1) return;
+    int ch = -1;
+    if (n <= kChain) {
+      for (int g = 0; g < n; ++g)
+        if (ch < 0 && j >= seg_lo[g]) ch = seg_ch[g];
+    } else {
+      int x = prev[i];
+      while (x != 0 && j < from[x]) x = prev[x];
+      ch = pch[x];
+    }
+    a = section_score(S, section_row(S, ch), q, j);
+    b = section_score(S, ri, q, j);
+  });
+}
+
 __device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScores& q) {
   constexpr int kGap = 1, kContained = 2, kSub = 3;
+  constexpr int kIterations = 4;         // parallel rounds before the ordered pass
+  constexpr int kOrdered = 1 << 30;      // stamp of a change made by the ordered pass
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
   const int* sec = S.sec;
   int* bl = S.bl;
   int* ed1 = reinterpret_cast<int*>(S.shared_tail);   // free until the smoothing
   int* prev = ed1 + kept;
   int* kind = prev + kept;
-  int* spec = kind + kept;
-  int* from = spec + kept;
-  int* until = from + kept;
-  auto row_at = [&](int k) { return section_row(S, sec[8 * k + 4]); };
-  // 1. Running maxima of the extended ends, first position on ties.
+  int* from = kind + kept;
+  int* stamp = from + kept;      // round of the last change of from[i]
+  int* computed = stamp + kept;  // round in which decision i was last taken
+  int* until = computed + kept;
+  int* pst = until + kept;       // position i's extended bounds and section
+  int* ped = pst + kept;
+  int* pch = ped + kept;
+  for (int i = threadIdx.x; i < kept; i += blockDim.x) {
+    const int o = sec[8 * i + 5];
+    pst[i] = bl[2 * o];
+    ped[i] = bl[2 * o + 1];
+    pch[i] = sec[8 * o + 4];
+  }
+  __syncthreads();
+  // 1. Running maxima of the extended ends (first position on ties), the
+  // merge kinds and the initial copy starts (each MergeF0Sub from st_i).
   if (warp == 0) {
-    int cv = bl[1], ci = 0;
+    int cv = ped[0], ci = 0, last_gap = 0;
     for (int i0 = 1; i0 < kept; i0 += 32) {
       const int i = i0 + lane;
-      const int e = i < kept ? bl[2 * i + 1] : INT_MIN;
+      const int e = i < kept ? ped[i] : INT_MIN;
       int v = e, x = i;
       for (int o = 1; o < 32; o <<= 1) {
         const int ov = __shfl_up_sync(kAll, v, o), ox = __shfl_up_sync(kAll, x, o);
@@ -936,9 +1004,15 @@ __device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScore
       if (lane == 0) pv = INT_MIN;
       const int mv = pv > cv ? pv : cv, mx = pv > cv ? px : ci;
       if (i < kept) {
+        const int st = pst[i];
+        const int kd = st > mv ? kGap : (e <= mv ? kContained : kSub);
         ed1[i] = mv;
         prev[i] = mx;
-        kind[i] = bl[2 * i] > mv ? kGap : (e <= mv ? kContained : kSub);
+        kind[i] = kd;
+        from[i] = kd == kContained ? -1 : st;
+        stamp[i] = -1;
+        computed[i] = -1;
+        if (kd == kGap) last_gap = i;
       }
       const int lv = __shfl_sync(kAll, v, 31), lx = __shfl_sync(kAll, x, 31);
       if (lv > cv) {
@@ -946,63 +1020,62 @@ __device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScore
         ci = lx;
       }
     }
-  }
-  __syncthreads();
-  // 2. Every MergeF0Sub decided against its p_i's values.
-  for (int i = 1 + warp; i < kept; i += warps) {
-    if (kind[i] != kSub) continue;
-    const SectionRow rp = row_at(prev[i]), ri = row_at(i);
-    const int lo = bl[2 * i], hi = ed1[i];
-    const bool larger = merge_sum_larger(lo, hi, [&](int j, double& a, double& b) {
-      a = b = 0.0;
-      if (j > hi) return;
-      a = section_score(S, rp, q, j);
-      b = section_score(S, ri, q, j);
-    });
-    if (lane == 0) spec[i] = larger;
-  }
-  __syncthreads();
-  // 3. The merges in order: copy starts, checked assumptions.
-  if (warp == 0) {
-    int st1 = bl[0];
-    for (int i0 = 1; i0 < kept; i0 += 32) {
-      const int i = i0 + lane;
-      int kd = 0, p = 0, sp = 0, st = 0, e1 = 0;
-      if (i < kept) {
-        kd = kind[i];
-        p = prev[i];
-        sp = kd == kSub ? spec[i] : 0;
-        st = bl[2 * i];
-        e1 = ed1[i];
-      }
-      const int m = imin(32, kept - i0);
-      for (int k = 0; k < m; ++k) {
-        const int kd_k = __shfl_sync(kAll, kd, k), p_k = __shfl_sync(kAll, p, k);
-        const int st_k = __shfl_sync(kAll, st, k), e1_k = __shfl_sync(kAll, e1, k);
-        bool larger = __shfl_sync(kAll, sp, k) != 0;
-        int fr = -1;
-        if (kd_k == kGap) {
-          fr = st_k;
-          st1 = st_k;
-        } else if (kd_k == kSub) {
-          if (p_k != 0 && from[p_k] > st_k) {
-            const SectionRow ri = row_at(i0 + k);
-            larger = merge_sum_larger(st_k, e1_k, [&](int j, double& a, double& b) {
-              a = b = 0.0;
-              if (j > e1_k) return;
-              int w = p_k;
-              while (w != 0 && j < from[w]) w = prev[w];
-              a = section_score(S, row_at(w), q, j);
-              b = section_score(S, ri, q, j);
-            });
-          }
-          fr = larger ? e1_k : st_k;
-        }
-        if (lane == 0) from[i0 + k] = fr;
-        __syncwarp();
-      }
+    // The reference leaves the running extent in boundary pair 0.
+    last_gap = __reduce_max_sync(kAll, last_gap);
+    const int st1 = last_gap > 0 ? pst[last_gap] : pst[0];
+    __syncwarp();
+    if (lane == 0) {
+      bl[0] = st1;
+      bl[1] = cv;
     }
-    // 4a. Where each copy ends: before the earliest later copy start.
+  }
+  __syncthreads();
+  // 2. Parallel rounds: each MergeF0Sub decided from the current copy
+  // starts, and again whenever one on its chain changed since.
+  bool settled = false;
+  for (int t = 0; t < kIterations && !settled; ++t) {
+    int mine = 0;   // this thread changed a copy start this round
+    for (int i = 1 + warp; i < kept; i += warps) {
+      if (kind[i] != kSub) continue;
+      const int st = pst[i], e1 = ed1[i];
+      bool fresh;
+      const bool larger = merge_decision(S, q, from, prev, stamp, pch, i, st, e1, t == 0, computed[i], fresh);
+      if (!fresh) continue;
+      const int fr = larger ? e1 : st;
+      if (lane == 0) {
+        computed[i] = t;
+        if (fr != from[i]) {
+          from[i] = fr;
+          stamp[i] = t;
+          mine = 1;
+        }
+      }
+      __syncwarp();
+    }
+    // One barrier that also tells every thread whether any changed.
+    settled = !__syncthreads_or(mine);
+  }
+  // 3. If the last round still changed something: the ordered pass, which
+  // decides again every decision a change on its chain may have reached.
+  if (!settled && warp == 0) {
+    for (int i = 1; i < kept; ++i) {
+      if (kind[i] != kSub) continue;
+      const int st = pst[i], e1 = ed1[i];
+      bool fresh;
+      const bool larger = merge_decision(S, q, from, prev, stamp, pch, i, st, e1, false, computed[i], fresh);
+      if (fresh) {
+        const int fr = larger ? e1 : st;
+        if (lane == 0 && fr != from[i]) {
+          from[i] = fr;
+          stamp[i] = kOrdered;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  // 4a. Where each copy ends: before the earliest later copy start.
+  if (warp == 0) {
     int carry = INT_MAX;
     for (int i1 = kept - 1; i1 >= 1; i1 -= 32) {
       const int i = i1 - lane;
@@ -1015,13 +1088,8 @@ __device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScore
       int later = __shfl_up_sync(kAll, v, 1);
       if (lane == 0) later = INT_MAX;
       later = imin(later, carry);
-      if (i >= 1 && f >= 0) until[i] = imin(bl[2 * i + 1], later == INT_MAX ? INT_MAX : later - 1);
+      if (i >= 1 && f >= 0) until[i] = imin(ped[i], later == INT_MAX ? INT_MAX : later - 1);
       carry = imin(carry, __shfl_sync(kAll, v, 31));
-    }
-    if (lane == 0) {
-      const int last = kept - 1;
-      bl[0] = st1;
-      bl[1] = kept > 1 ? imax(ed1[last], bl[2 * last + 1]) : bl[1];
     }
   }
   __syncthreads();
@@ -1030,7 +1098,7 @@ __device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScore
     const int fr = from[i];
     if (fr < 0) continue;
     const int to = until[i];
-    const SectionRow r = row_at(i);
+    const SectionRow r = section_row(S, pch[i]);
     for (int j = fr + lane; j <= to; j += 32) S.s3[j] = r.value(S.s2, j);
   }
   __syncthreads();
@@ -1197,14 +1265,15 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
       }
   }
   __syncthreads();
-  if (kept != 0 && sorted) {
+  // The parallel merge needs section 0 first in the sorted order.
+  if (kept != 0 && sec[5] == 0) {
     const SectionRow first = section_row(S, sec[4]);
     for (int j = tid; j < F; j += nt) S.s3[j] = first.value(S.s2, j);
     merge_sorted(S, kept, MergeScores{cand, score, stride, columns});
   } else if (kept != 0) {
     // MergeF0 (harvest.cpp:937-963) in the reference's order, when
-    // MakeSortedOrder reorders the sections: start from the first kept
-    // section (every thread), then warp 0 merges in sorted order. ms[j] holds the
+    // MakeSortedOrder moves kept section 0 from first place: start from
+    // section 0 (every thread), then warp 0 merges in sorted order. ms[j] holds the
     // SearchScore of merged frame j's value where contour_extend recorded it
     // and NaN where it did not (a SearchScore is never NaN); MergeF0Sub's
     // sums compute the missing ones.
