@@ -26,10 +26,12 @@ constexpr int kZone = 100;             // body frames at each end whose SearchSc
 
 // Doubles of scratch one clip of `frames` frames needs (contour_adjoint
 // reuses the same space with a layout of its own).
-__host__ __device__ inline int64_t contour_scratch_doubles(int64_t frames) {
+// `threads`: the block size contour_finish runs with (per-thread smoothing
+// tails, per-warp long buffers).
+__host__ __device__ inline int64_t contour_scratch_doubles(int64_t frames, int threads) {
   const int64_t cap = (frames + 1) / 8 + 2;   // voiced sections: runs of >= 7 frames
   return 4 * frames + 4 * kExtend * cap + 2 * kZone * cap + 4 * cap + (frames + 602) +
-         int64_t(kContourThreads) * kTransient + kContourWarps * (frames + 600) + (frames + 602) / 2 +
+         int64_t(threads) * kTransient + (threads / 32) * (frames + 600) + (frames + 602) / 2 +
          frames + 8 + 64;
 }
 
@@ -42,13 +44,13 @@ struct ContourScratch {
   int* sec;                    // [cap][8] st, ed, extended st, extended ed, kept section, order,
                                //          frames examined backward, forward
   int* bl;                     // boundary lists, up to 2 (F + 602) ints
-  double* tails;               // kContourThreads x kTransient smoothing tails
-  double* shared_tail;         // kContourWarps x (F + 600)
+  double* tails;               // threads x kTransient smoothing tails
+  double* shared_tail;         // warps x (F + 600)
   int* deferred;               // sections whose tail needs the long buffer
   double* ms;                  // [F] recorded SearchScore of merged frame j's value, NaN if none
   int* meta;                   // [0] sections, [1] kept sections
   int64_t cap;
-  __device__ ContourScratch(double* sc, int F) {
+  __device__ ContourScratch(double* sc, int F, int threads) {
     cap = (F + 1) / 8 + 2;
     s1 = sc;
     s2 = s1 + F;
@@ -60,8 +62,8 @@ struct ContourScratch {
     sec = reinterpret_cast<int*>(zone_sc + 2 * kZone * cap);
     bl = sec + 8 * cap;
     tails = reinterpret_cast<double*>(bl) + (F + 602);
-    shared_tail = tails + static_cast<int64_t>(kContourThreads) * kTransient;
-    deferred = reinterpret_cast<int*>(shared_tail + static_cast<int64_t>(kContourWarps) * (F + 600));
+    shared_tail = tails + static_cast<int64_t>(threads) * kTransient;
+    deferred = reinterpret_cast<int*>(shared_tail + static_cast<int64_t>(threads / 32) * (F + 600));
     ms = reinterpret_cast<double*>(deferred + 2 * ((F + 602) / 2));
     meta = reinterpret_cast<int*>(ms + F);
   }
@@ -560,17 +562,18 @@ __device__ void smooth_section_warp(P padded, int st, int ed, int64_t len, doubl
 //                    ExtendF0 runs of every section, recording with every
 //                    value it writes that value's SearchScore, and the
 //                    SearchScore of the first and last kZone body frames;
-//   contour_finish   (a block of 8 warps per clip): ExtendSub's carried
-//                    mean and MergeF0 in order on warp 0 (MergeF0Sub's score
-//                    sums read the recorded SearchScores), FixStep4,
-//                    SmoothF0Contour and the resampling.
+//   contour_finish   (a block of 8 or 16 warps per clip): ExtendSub's
+//                    carried mean, MergeF0 (in parallel when the sections
+//                    come sorted; MergeF0Sub's score sums read the recorded
+//                    SearchScores), FixStep4, SmoothF0Contour and the
+//                    resampling.
 __global__ void __launch_bounds__(kContourThreads) contour_prepare(ContourView v) {
   __shared__ int red[kContourWarps];
   const int c = blockIdx.x, tid = threadIdx.x, nt = blockDim.x;
   const BatchView& B = v.batch;
   const int64_t row0 = B.frame_off[c];
   const int F = static_cast<int>(B.frame_off[c + 1] - row0);
-  const ContourScratch S(v.scratch + v.scratch_off[c], F);
+  const ContourScratch S(v.scratch + v.scratch_off[c], F, v.finish_threads);
   const double* base = v.best + row0;
   // FixStep1 (harvest.cpp:710-722), allowed range 0.008.
   for (int i = tid; i < F; i += nt) {
@@ -814,7 +817,7 @@ __global__ void __launch_bounds__(kContourThreads, 2) contour_extend(ContourView
   const int stride = B.capacity;
   const double* cand = v.pruned + row0 * stride;
   const double* score = v.pruned_scores + row0 * stride;
-  const ContourScratch S(v.scratch + v.scratch_off[c], F);
+  const ContourScratch S(v.scratch + v.scratch_off[c], F, v.finish_threads);
   const int sections = S.meta[0];
   for (int i = gw; i < sections; i += nw) {
     if (columns <= 128) extend_section<4, 4, 4>(S, i, F, cand, score, stride, columns);
@@ -878,7 +881,8 @@ __device__ bool merge_sum_larger(int lo, int hi, Fetch fetch) {
 }
 
 // MergeF0 (harvest.cpp:937-963) in parallel, for a sort order (sec[8i + 5],
-// from MakeSortedOrder) that keeps kept section 0 first: the reference reads
+// from MakeSortedOrder) that leaves the extended starts non-decreasing and
+// keeps kept section 0 first: the reference reads
 // position i's bounds from boundary pair order[i], which aliases the running
 // extent (pair 0) only for section 0, and starts the merged contour from
 // section 0. Position i stands for kept section order[i]. With
@@ -1104,8 +1108,13 @@ __device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScore
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v) {
-  __shared__ int red[kContourWarps];
+// kThreads: 256, or 512 when the batch has fewer clips than the GPU has SMs
+// (one block per clip, so the larger block only adds warps to the
+// block-parallel parts: ExtendSub's sums, MergeF0's decisions, smoothing).
+template <int kThreads>
+__global__ void __launch_bounds__(kThreads) contour_finish(ContourView v) {
+  constexpr int kWarps = kThreads / 32;
+  __shared__ int red[kWarps];
   __shared__ int deferred_count;
   const int c = blockIdx.x;
   const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -1116,7 +1125,7 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
   const int stride = B.capacity;
   const double* cand = v.pruned + row0 * stride;
   const double* score = v.pruned_scores + row0 * stride;
-  const ContourScratch S(v.scratch + v.scratch_off[c], F);
+  const ContourScratch S(v.scratch + v.scratch_off[c], F, v.finish_threads);
   const int sections = S.meta[0];
   int* sec = S.sec;
   int* bl = S.bl;
@@ -1265,15 +1274,25 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
       }
   }
   __syncthreads();
-  // The parallel merge needs section 0 first in the sorted order.
-  if (kept != 0 && sec[5] == 0) {
+  // The parallel merge needs the order MakeSortedOrder produced to keep
+  // section 0 first and to leave the extended starts non-decreasing: its
+  // insertion sort swaps order[i] with order[j] rather than shifting, so its
+  // result need not be sorted.
+  bool parallel = sorted;
+  if (!sorted) {
+    int bad = 0;
+    for (int k = tid; k + 1 < kept; k += nt) bad |= bl[2 * sec[8 * k + 5]] > bl[2 * sec[8 * (k + 1) + 5]];
+    parallel = !__syncthreads_or(bad) && sec[5] == 0;
+  }
+  if (kept != 0 && parallel) {
     const SectionRow first = section_row(S, sec[4]);
     for (int j = tid; j < F; j += nt) S.s3[j] = first.value(S.s2, j);
     merge_sorted(S, kept, MergeScores{cand, score, stride, columns});
   } else if (kept != 0) {
     // MergeF0 (harvest.cpp:937-963) in the reference's order, when
-    // MakeSortedOrder moves kept section 0 from first place: start from
-    // section 0 (every thread), then warp 0 merges in sorted order. ms[j] holds the
+    // MakeSortedOrder moves kept section 0 from first place or leaves the
+    // starts unsorted: start from section 0 (every thread), then warp 0
+    // merges in that order. ms[j] holds the
     // SearchScore of merged frame j's value where contour_extend recorded it
     // and NaN where it did not (a SearchScore is never NaN); MergeF0Sub's
     // sums compute the missing ones.
@@ -1436,7 +1455,7 @@ __global__ void __launch_bounds__(kContourThreads) contour_finish(ContourView v)
   int long_index = 0;
   for (int s = 0; s < nbs / 2; ++s)
     if (bl[2 * s + 1] - bl[2 * s] + 1 >= kLongSection) {
-      if (long_index % kContourWarps == warp)
+      if (long_index % kWarps == warp)
         smooth_section_warp(padded, bl[2 * s], bl[2 * s + 1], len, sm, S.shared_tail + warp * (F + 600), len);
       ++long_index;
     }
@@ -1594,7 +1613,8 @@ cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream) {
 cudaError_t launch_contour(const ContourView& v, cudaStream_t stream) {
   contour_prepare<<<v.batch.clips, kContourThreads, 0, stream>>>(v);
   contour_extend<<<dim3(v.batch.clips, v.extend_blocks > 1 ? v.extend_blocks : 1), kContourThreads, 0, stream>>>(v);
-  contour_finish<<<v.batch.clips, kContourThreads, 0, stream>>>(v);
+  if (v.finish_threads == 512) contour_finish<512><<<v.batch.clips, 512, 0, stream>>>(v);
+  else contour_finish<kContourThreads><<<v.batch.clips, kContourThreads, 0, stream>>>(v);
   return cudaGetLastError();
 }
 
@@ -1628,6 +1648,6 @@ cudaError_t launch_search_base(const double* cand, const double* scores, int64_t
   return cudaGetLastError();
 }
 
-int64_t contour_scratch(int64_t frames) { return contour_scratch_doubles(frames); }
+int64_t contour_scratch(int64_t frames, int finish_threads) { return contour_scratch_doubles(frames, finish_threads); }
 
 }  // namespace hv

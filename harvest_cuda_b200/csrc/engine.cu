@@ -216,6 +216,9 @@ struct Plan {
   RefineShape refine_shape;
   int extend_blocks = 0;
   bool tuned = false;
+  // contour_finish's block size: 512 when the batch has fewer clips than
+  // the GPU has SMs (a block per clip), else 256.
+  int contour_threads = 256;
   // Captured launch sequence for this plan at a given arena base.
   cudaGraphExec_t graph = nullptr;
   void* graph_arena = nullptr;
@@ -437,6 +440,7 @@ struct Workspace {
     p->s = s;
     p->lengths = std::move(lengths);
     const int B = p->clips = static_cast<int>(p->lengths.size());
+    p->contour_threads = B < sms ? 512 : 256;
     p->ratio = ratio_for(s.fs);
     p->fs_r = double(s.fs) / p->ratio;
     p->bank = bank_for(s);
@@ -462,7 +466,7 @@ struct Workspace {
       p->seg_off[c + 1] = p->seg_off[c] + (p->ratio > 1 ? (total + kSegment - 1) / kSegment : 0);
       p->frame_off[c + 1] = p->frame_off[c] + frames;
       p->out_off[c + 1] = p->out_off[c] + samples_for(s.fs, n, s.period);
-      p->scratch_off[c + 1] = p->scratch_off[c] + contour_scratch(frames);
+      p->scratch_off[c + 1] = p->scratch_off[c] + contour_scratch(frames, p->contour_threads);
       p->nfft[c] = suitable_fft_size(y_len + 5 + 2 * static_cast<int>(2.0 * p->fs_r / first));
       p->slot_capacity = std::max<int64_t>(p->slot_capacity, y_len / 2 + 2);
     }
@@ -624,6 +628,7 @@ struct Workspace {
     int64_t longest = 0;
     for (int c = 0; c < p.clips; ++c) longest = std::max(longest, p.frame_off[c + 1] - p.frame_off[c]);
     cv.extend_blocks = p.extend_blocks > 0 ? p.extend_blocks : contour_extend_blocks(longest);
+    cv.finish_threads = p.contour_threads;
     return cv;
   }
 
@@ -1447,8 +1452,10 @@ int hv_contour_batch(const double* f0_candidates, const double* scores, const do
     else if (on_device && (flags & HV_NULL_IS_LEGACY_STREAM)) st = cudaStreamLegacy;
     // Host tables: scratch offsets per clip, columns per clip.
     std::vector<int64_t> scratch_off(clips + 1, 0);
+    const int finish_threads = clips < ws.sms ? 512 : 256;
     for (int c = 0; c < clips; ++c)
-      scratch_off[c + 1] = scratch_off[c] + contour_scratch(frame_offsets[c + 1] - frame_offsets[c]);
+      scratch_off[c + 1] =
+          scratch_off[c] + contour_scratch(frame_offsets[c + 1] - frame_offsets[c], finish_threads);
     std::vector<int> cols(clips, columns);
     // Workspace buffer: [frame offsets | scratch offsets | columns | base |
     // scratch | (host inputs: candidates, scores) | (host outputs: fixed,
@@ -1508,6 +1515,7 @@ int hv_contour_batch(const double* f0_candidates, const double* scores, const do
     int64_t longest = 0;
     for (int c = 0; c < clips; ++c) longest = std::max(longest, frame_offsets[c + 1] - frame_offsets[c]);
     cv.extend_blocks = contour_extend_blocks(longest);
+    cv.finish_threads = finish_threads;
     check(launch_contour(cv, st), "contour");
     if (!on_device) {
       if (fixed)

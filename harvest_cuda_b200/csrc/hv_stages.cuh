@@ -69,6 +69,7 @@ struct ContourView {
   int column_multiple;          // candidate columns of clip c: column_multiple * count[c]
   double* fixed_out;            // [frames] FixF0Contour's result, when not null
   int extend_blocks;            // blocks per clip of the section-extension kernel
+  int finish_threads;           // block size of contour_finish (256 or 512); sizes the scratch
 };
 
 // Blocks per clip of the contour's section-extension kernel for a batch
@@ -193,7 +194,7 @@ cudaError_t launch_prune(const BatchView& v, const double* refined, const double
                          const int* count, int64_t total_frames, double* pruned,
                          double* pruned_scores, double* best, cudaStream_t stream);
 
-int64_t contour_scratch(int64_t frames);
+int64_t contour_scratch(int64_t frames, int finish_threads);
 cudaError_t launch_tape(const ContourView& v, const double* cand, int64_t total_frames, double* tape,
                         cudaStream_t stream);
 cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream);

@@ -40,6 +40,18 @@ def test_batch_graph_and_stagewise_agree(gpu):
         np.testing.assert_array_equal(u, v)
 
 
+def test_contour_block_size_does_not_change_f0(gpu):
+    # A batch with at least as many clips as the GPU has SMs (148 on a B200)
+    # runs the contour's last kernel with 256 threads per clip, a smaller one
+    # with 512; both must give the same F0 for every clip.
+    clips, _ = signals.ragged_batch(200, 16000, (0.3, 1.2), seed=21)
+    big = hv.harvest_many(clips, 16000, 50.0, 1100.0, 5.0)
+    small = hv.harvest_many(clips[:9], 16000, 50.0, 1100.0, 5.0)
+    for (f0, t), (g0, u) in zip(big[:9], small):
+        np.testing.assert_array_equal(f0, g0)
+        np.testing.assert_array_equal(t, u)
+
+
 def test_batch_matches_checker(gpu, checker):
     clips = _clips(count=6, seed=11)
     out = hv.harvest_many(clips, 16000, 50.0, 1100.0, 5.0)
