@@ -29,7 +29,7 @@ __device__ __forceinline__ int size_class(int len) {
 // Only those bins are needed, so they are evaluated directly as DFT sums.
 // The window phasor advances by 2 pi / len per sample and each twiddle by
 // 2 pi k / n; both are re-anchored from exact values every kAnchor samples.
-constexpr int kAnchor = 64;
+constexpr int kAnchor = 256;
 
 // The discrete parameters of one candidate's refinement: window half length,
 // FFT size, first waveform index and the harmonic bins.
@@ -369,10 +369,10 @@ __device__ __forceinline__ void candidate_spectra(const double* __restrict__ y, 
   // Between anchors the window cosine follows the Chebyshev recurrence
   // cos((k + 1) d) = 2 cos d cos(k d) - cos((k - 1) d): one multiply-add per
   // sample instead of a four-operation rotation. Its rounding error grows
-  // as k / sin d over the 64 samples between exact anchors: at most about
-  // 5e-13 of the window, at the longest windows (483 samples, d = 2 pi /
-  // 483), far below the F0 tolerance; the refined F0 moves by a few 1e-14
-  // relative.
+  // as k / sin d over the 256 samples between exact anchors: at most about
+  // 2e-12 of the window, at the longest windows (483 samples, d = 2 pi /
+  // 483), far below the F0 tolerance; the refined F0 moves by about 1e-13
+  // relative (against anchors every 64 samples, on the 16 kHz batch).
   const double k2 = 2.0 * dc;
   for (int i0 = 0; i0 < len - 1; i0 += kAnchor) {
     phase(i0 + 1, nc, ns);
