@@ -619,7 +619,7 @@ def run_ours(args):
     if rank == 0:
         line = summarize(args, wl, value, ms, stages, e2e, clocks.summary(), local, world)
         line["autotuned"] = {"refine_min_blocks_per_sm": tuning[0], "refine_grid_blocks_per_sm": tuning[1],
-                             "key": "fs, f0 range, log2 of the batch's samples"}
+                             "key": "fs, f0 range, log2 of the batch's samples, log2 of its longest clip's frames"}
         if world == 1 and not args.no_per_clip:
             line["per_clip"] = per_clip(hv, wl, local)
             line["batched_over_per_clip"] = round(e2e["value"] / line["per_clip"]["value"], 2)

@@ -105,8 +105,9 @@ HV_API int hv_profile(const double* x, int64_t n, int fs, double f0_floor, doubl
                double* stage_ms);
 
 /* Refinement launch shape of the calling thread's last Harvest call (no
- * reference counterpart). The engine autotunes it once per (fs, f0_floor,
- * f0_ceil, log2 of the batch's total samples) on each device, the first time
+ * reference counterpart). The engine autotunes it, with the contour's
+ * extension blocks, once per (fs, f0_floor, f0_ceil, log2 of the batch's
+ * total samples, log2 of its longest clip's frames) on each device, the first time
  * a batch with that key runs, by timing every candidate shape on that
  * batch; all shapes give bit-identical results. shape[0]: minimum resident
  * 128-thread blocks per SM of the kernel instance (1, 4 or 5), shape[1]:
