@@ -189,3 +189,39 @@ def test_extend_sub_decisions_on_the_threshold(gpu, checker):
         trials.append((np.zeros((frames, 8)), np.zeros((frames, 8)), base))
     results = run_batch(trials, use_base=True)
     expect_equal(checker, trials, results, use_base=True)
+
+
+def dense_trial(rng, trial):
+    """Short given sections every few dozen frames, with every track holding
+    one of two pitches at every frame, so that each section extends up to
+    100 frames both ways and several extended sections overlap at once:
+    MergeF0's decisions then depend on one another through long chains."""
+    frames = 3000 + int(rng.integers(3000))
+    pitches = (120.0, 150.0) if trial % 2 else (200.0, 203.0)
+    cand = np.zeros((frames, 8))
+    scores = np.zeros((frames, 8))
+    for col in range(8):
+        cand[:, col] = pitches[col % 2]
+        scores[:, col] = 1 + rng.integers(10, size=frames)
+    base = np.zeros(frames)
+    start = 1 + int(rng.integers(20))
+    while start < frames - 2:
+        end = min(frames - 2, start + 7 + int(rng.integers(30)))
+        base[start:end + 1] = pitches[int(rng.integers(2))]
+        start = end + 2 + int(rng.integers(25))
+    return cand, scores, base
+
+
+@pytest.mark.parametrize("use_base", [False, True], ids=["search_f0_base", "given_base"])
+def test_dense_overlapping_sections(gpu, checker, use_base):
+    rng = np.random.default_rng(4242)
+    trials = [dense_trial(rng, t) for t in range(60)]
+    results = run_batch(trials, use_base)
+    for k, ((cand, scores, base), (fixed, smoothed)) in enumerate(zip(trials, results)):
+        want = checker.fix_contour(cand, scores, base=base if use_base else None)
+        np.testing.assert_array_equal(fixed, want, err_msg=f"FixF0Contour, trial {k}")
+        # Merged sections here reach 2048 frames and more, which the engine
+        # smooths a warp at a time: equal to WORLD's pass up to rounding.
+        np.testing.assert_allclose(smoothed, checker.smooth_contour(want), rtol=1e-12, atol=0,
+                                   err_msg=f"SmoothF0Contour, trial {k}")
+    assert sum(int(np.count_nonzero(f)) for f, _ in results) > 100000
