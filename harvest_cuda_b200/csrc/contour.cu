@@ -18,6 +18,10 @@ namespace hv {
 
 constexpr int kExtend = 101;      // ExtendF0 writes at most 101 frames per side
 constexpr int kTransient = 1024;  // per-lane buffer for a smoothing tail
+// Free-response steps the smoothing adjoint follows past a section's ends:
+// the filter's poles have radius 0.875, so the rest is below 0.875^512
+// (1e-30) of the response's peak.
+constexpr int kAdjointTail = 512;
 constexpr unsigned kAll = 0xffffffffu;
 
 constexpr int kContourThreads = 256;   // threads of a clip's block in contour_prepare / contour_finish
@@ -1508,8 +1512,8 @@ __global__ void record_tape(ContourView v, const double* __restrict__ cand, int6
 //     padding, Butterworth pass, reversal, pass, reversal); its transpose is
 //     the same two passes over the section's gradient, zero outside it,
 //     followed by summing the held regions into the section's end frames.
-//     The free response beyond kTransient samples past either end
-//     (below 0.88^1024 of the peak) is dropped;
+//     The free response beyond kAdjointTail samples past either end
+//     (below 0.875^512 of the peak) is dropped;
 //   * FixStep4: a frame filled cnt frames into a gap of d frames between
 //     sections ending at a and starting at b depends on the step-3 values
 //     at a and b with weights 1 - cnt / (d + 1) and cnt / (d + 1).
@@ -1566,7 +1570,7 @@ __global__ void __launch_bounds__(32) contour_adjoint(GradView v) {
     Butter fw;
     for (int j = st; j <= ed; ++j) body[j - lag] = fw.step(g_sm[j - lag]);
     double* tail = tails + lane * kTransient;
-    const int64_t trailing = len - 1 - ed < kTransient ? len - 1 - ed : kTransient;
+    const int64_t trailing = len - 1 - ed < kAdjointTail ? len - 1 - ed : kAdjointTail;
     for (int64_t k = 0; k < trailing; ++k) tail[k] = fw.step(0.0);
     Butter bw;
     double held = 0.0;
@@ -1574,7 +1578,7 @@ __global__ void __launch_bounds__(32) contour_adjoint(GradView v) {
     for (int j = ed; j >= st; --j) g_s4[j - lag] = bw.step(body[j - lag]);
     g_s4[ed - lag] += held;
     held = 0.0;
-    const int leading = st < kTransient ? st : kTransient;
+    const int leading = st < kAdjointTail ? st : kAdjointTail;
     for (int k = 0; k < leading; ++k) held += bw.step(0.0);
     g_s4[st - lag] += held;
   }
