@@ -98,8 +98,9 @@ __global__ void decimate_chain(DecimateView v, const double* __restrict__ z, int
   entry[3 * seg + 2] = s2;
 }
 
-// Pass 0 writes the forward output u; pass 1 writes the kept samples of the
-// backward output into y (before DC removal).
+// The backward pass (kPass 1): writes the kept samples of the backward
+// output into y (before DC removal). The forward pass is
+// decimate_forward_staged, below.
 constexpr int kDecimateThreads = 128;
 
 template <int kPass>
@@ -112,13 +113,6 @@ __global__ void decimate_segment_run(DecimateView v, const double* __restrict__ 
   int64_t total = v.t_off[c + 1] - v.t_off[c];
   double* uc = u + v.t_off[c];
   double s0 = states[3 * seg], s1 = states[3 * seg + 1], s2 = states[3 * seg + 2];
-  if (kPass == 0) {
-    const double* xc = x + v.x_off[c];
-    const int64_t n = v.x_off[c + 1] - v.x_off[c];
-    const int lag = v.lag;
-    for (int64_t i = begin; i < end; ++i) uc[i] = lowpass_step(v, forward_input(xc, n, lag, i), s0, s1, s2);
-    return;
-  }
   // Kept sample k of the decimated clip sits at backward index
   // total - 9 - nbeg - (skip + k) * r (matlabfunctions.cpp:195-200).
   const int r = v.ratio;
@@ -337,6 +331,48 @@ __global__ void remove_mean_and_edge_bins(const BatchView v, double* __restrict_
   }
 }
 
+// Pass 0 with coalesced stores: each thread runs its own segment, 32 steps
+// at a time, into its row of a shared tile; each warp then stores its 32
+// threads' rows, each row one contiguous run of u. Every thread of the block
+// takes part in every barrier.
+__global__ void __launch_bounds__(kDecimateThreads)
+decimate_forward_staged(DecimateView v, const double* __restrict__ x, double* __restrict__ u, int64_t segments,
+                        const double* __restrict__ states) {
+  __shared__ double tile[kDecimateThreads][33];
+  __shared__ long long base[kDecimateThreads];
+  __shared__ int length[kDecimateThreads];
+  const int t = threadIdx.x, w = t >> 5, lane = t & 31;
+  const int64_t seg = blockIdx.x * (int64_t)blockDim.x + t;
+  const bool live = seg < segments;
+  int c = 0;
+  int64_t begin = 0, end = 0, n = 0;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0;
+  const double* xc = x;
+  if (live) {
+    clip_of_segment(v, seg, c, begin, end);
+    s0 = states[3 * seg];
+    s1 = states[3 * seg + 1];
+    s2 = states[3 * seg + 2];
+    xc = x + v.x_off[c];
+    n = v.x_off[c + 1] - v.x_off[c];
+  }
+  base[t] = live ? v.t_off[c] + begin : 0;
+  length[t] = live ? static_cast<int>(end - begin) : 0;
+  const int lag = v.lag;
+  for (int t0 = 0; t0 < v.seg_len; t0 += 32) {
+    for (int k = 0; k < 32; ++k) {
+      const int64_t i = begin + t0 + k;
+      if (live && i < end) tile[t][k] = lowpass_step(v, forward_input(xc, n, lag, i), s0, s1, s2);
+    }
+    __syncthreads();
+    for (int r = 0; r < 32; ++r) {
+      const int row = 32 * w + r;
+      if (t0 + lane < length[row]) u[base[row] + t0 + lane] = tile[row][lane];
+    }
+    __syncthreads();
+  }
+}
+
 // Host-side launchers -------------------------------------------------------
 
 // `states` holds 6 doubles per segment: the zero-state results, then the
@@ -348,7 +384,7 @@ cudaError_t launch_decimate(const DecimateView& v, const double* x, double* u, d
   double* entry = states + 3 * segments;
   decimate_segment_states<0><<<grid, threads, 0, stream>>>(v, x, u, segments, states);
   decimate_chain<<<grid, threads, 0, stream>>>(v, states, segments, entry);
-  decimate_segment_run<0><<<grid, threads, 0, stream>>>(v, x, u, segments, entry, y);
+  decimate_forward_staged<<<grid, threads, 0, stream>>>(v, x, u, segments, entry);
   decimate_segment_states<1><<<grid, threads, 0, stream>>>(v, x, u, segments, states);
   decimate_chain<<<grid, threads, 0, stream>>>(v, states, segments, entry);
   decimate_segment_run<1><<<grid, threads, 0, stream>>>(v, x, u, segments, entry, y);
@@ -365,7 +401,7 @@ cudaError_t preload_decimation_kernels() {
   load(reinterpret_cast<const void*>(decimate_segment_states<0>));
   load(reinterpret_cast<const void*>(decimate_segment_states<1>));
   load(reinterpret_cast<const void*>(decimate_chain));
-  load(reinterpret_cast<const void*>(decimate_segment_run<0>));
+  load(reinterpret_cast<const void*>(decimate_forward_staged));
   load(reinterpret_cast<const void*>(decimate_segment_run<1>));
   load(reinterpret_cast<const void*>(copy_clips));
   load(reinterpret_cast<const void*>(remove_mean_and_edge_bins));
