@@ -12,7 +12,7 @@
 // for bit, except for the smoothing of sections of 2048 frames or more.
 #include <math_constants.h>
 
-#include "hv_stages.cuh"
+#include "hv_events.cuh"   // block_scan_packed (and hv_stages.cuh)
 
 namespace hv {
 
@@ -1146,9 +1146,9 @@ __global__ void __launch_bounds__(kThreads) contour_finish(ContourView v) {
   // order) / n_i and the running mean is never reset. Only the decisions
   // are used. Each warp first sums its sections' values in any order; with
   // every value nonnegative, that sum and the reference's ordered one are
-  // both within (n_i + 1) u relative of the exact sum. Thread 0 then runs
-  // the recurrence on the warps' sums, carrying a bound on the relative
-  // error of its mean and of the reference's, and takes a decision only if
+  // both within (n_i + 1) u relative of the exact sum. The recurrence then
+  // runs on those sums (below), carrying a bound on the relative error of
+  // its mean and of the reference's, and takes a decision only if
   // 2200 / mean lies farther from n_i than that bound can move it. If any
   // decision is that close, or any value is negative or not finite, warp 0
   // repeats the reference's ordered sum exactly. Kept sections keep their
@@ -1158,6 +1158,8 @@ __global__ void __launch_bounds__(kThreads) contour_finish(ContourView v) {
   __shared__ int unsafe;
   if (tid == 0) unsafe = 0;
   __syncthreads();
+  __shared__ double warp_max[kWarps];
+  double vmax = 0.0;
   for (int i = warp; i < sections; i += nt / 32) {
     const SectionRow r = section_row(S, i);
     const int st = sec[8 * i + 2], ed = sec[8 * i + 3];
@@ -1167,6 +1169,7 @@ __global__ void __launch_bounds__(kThreads) contour_finish(ContourView v) {
       const double x = r.value(S.s2, j);
       bad |= !(x >= 0.0 && x <= 1.0e300);
       part += x;
+      vmax = fmax(vmax, x);
     }
     for (int o = 16; o; o >>= 1) part += __shfl_xor_sync(kAll, part, o);
     if (__any_sync(kAll, bad) && lane == 0) unsafe = 1;
@@ -1175,37 +1178,61 @@ __global__ void __launch_bounds__(kThreads) contour_finish(ContourView v) {
       sums[2 * i + 1] = ed - st;
     }
   }
+  for (int o = 16; o; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(kAll, vmax, o));
+  if (lane == 0) warp_max[warp] = vmax;
   __syncthreads();
-  if (tid == 0 && !unsafe) {
+  // Each thread takes sections; section i's mean is the recurrence run over
+  // the last kWindow sections from a zero mean. With every n >= 2 (else the
+  // exact path runs) a mean never exceeds twice the largest value, so the
+  // mean carried into the window adds at most (2 max value) times the
+  // product of 1/n over the window, below 1e-20 of the mean on real
+  // sections; that bound joins the carried rounding bound. Sections within
+  // kWindow of the start run the whole recurrence, in the same order.
+  if (!unsafe) {
     constexpr double u = 1.1102230246251565e-16;   // 2^-53
-    int kept = 0;
-    double mean = 0.0, err = 0.0;
-    // Eight sections' sums and lengths are loaded before they are used.
-    for (int i0 = 0; i0 < sections && !unsafe; i0 += 8) {
-      double sm[8], nn[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        sm[q] = i0 + q < sections ? sums[2 * (i0 + q)] : 0.0;
-        nn[q] = i0 + q < sections ? sums[2 * (i0 + q) + 1] : 1.0;
-      }
-#pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        if (i0 + q >= sections || unsafe) break;
-        const double n = nn[q];
-        const double sum = mean + sm[q];
+    constexpr int kWindow = 32;
+    double top = 0.0;
+    for (int w = 0; w < kWarps; ++w) top = fmax(top, warp_max[w]);
+    int* keep = reinterpret_cast<int*>(sums + 2 * static_cast<int64_t>(sections));
+    for (int i = tid; i < sections; i += nt) {
+      const int k0 = imax(0, i - kWindow + 1);
+      double mean = 0.0, err = 0.0, carried = 1.0, sum = 0.0;
+      bool ok = true;
+      for (int k = k0; k <= i; ++k) {
+        const double n = sums[2 * k + 1];
+        ok &= n >= 2.0;
+        sum = mean + sums[2 * k];
         const double rho = sum > 0.0 ? mean / sum : 0.0;
         err = err * rho + (n + 3.0) * u * 1.0001;
         mean = sum / n;
-        if (sum == 0.0) continue;                     // exactly zero for both: never kept
-        const double ratio = 2200.0 / mean;
-        if (!(fabs(ratio - n) > ratio * (4.0 * err + 8.0 * u))) {
-          unsafe = 1;
-          break;
-        }
-        if (ratio < n) sec[8 * kept++ + 4] = i0 + q;
+        carried /= n;
       }
+      int decision = 0;
+      if (!ok) unsafe = 1;                            // the bound below needs every n >= 2
+      if (sum != 0.0) {                               // exactly zero for both: never kept
+        const double n = sums[2 * i + 1];
+        const double ratio = 2200.0 / mean;
+        const double bound = err + (k0 > 0 ? 2.01 * top * carried / mean : 0.0);
+        if (!(fabs(ratio - n) > ratio * (4.0 * bound + 8.0 * u))) unsafe = 1;
+        else decision = ratio < n;
+      }
+      keep[i] = decision;
     }
-    if (!unsafe) S.meta[1] = kept;
+    __syncthreads();
+    if (!unsafe) {
+      // Kept sections in order: a block scan of the flags, a block at a time.
+      __shared__ unsigned long long scan_scratch[kWarps];
+      int running = 0;
+      for (int b0 = 0; b0 < sections; b0 += nt) {
+        const int i = b0 + tid;
+        const unsigned long long f = i < sections && keep[i] ? 1ull : 0ull;
+        unsigned long long total;
+        const unsigned long long before = block_scan_packed(f, scan_scratch, total);
+        if (f) sec[8 * (running + static_cast<int>(before)) + 4] = i;
+        running += static_cast<int>(total);
+      }
+      if (tid == 0) S.meta[1] = running;
+    }
   }
   __syncthreads();
   // The exact ordered sum, when a decision was too close to call: warp 0
