@@ -1039,11 +1039,17 @@ __device__ void merge_sorted(const ContourScratch& S, int kept, const MergeScore
   }
   __syncthreads();
   // 2. Parallel rounds: each MergeF0Sub decided from the current copy
-  // starts, and again whenever one on its chain changed since.
+  // starts, and again whenever one on its chain changed since. Each warp
+  // takes a contiguous run of positions and walks it in order, so a chain
+  // inside the run sees the copy starts its warp has just set (p_i is
+  // nearly always one or two positions back); only chains reaching into
+  // another warp's run can need a later round.
   bool settled = false;
+  const int per_warp = (kept - 1 + warps - 1) / warps;
+  const int run_lo = 1 + warp * per_warp, run_hi = imin(kept, run_lo + per_warp);
   for (int t = 0; t < kIterations && !settled; ++t) {
     int mine = 0;   // this thread changed a copy start this round
-    for (int i = 1 + warp; i < kept; i += warps) {
+    for (int i = run_lo; i < run_hi; ++i) {
       if (kind[i] != kSub) continue;
       const int st = pst[i], e1 = ed1[i];
       bool fresh;
