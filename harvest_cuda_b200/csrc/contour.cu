@@ -952,26 +952,19 @@ __device__ __forceinline__ bool merge_decision(const ContourScratch& S, const Me
   }
   if (!fresh) return false;
   const SectionRow ri = section_row(S, pch[i]);
-  // The newest writer's row is held; older writers' rows (frames before its
-  // copy start) are formed per frame.
-  const SectionRow r0 = section_row(S, seg_ch[0]);
   return merge_sum_larger(st, e1, [&](int j, double& a, double& b) {
     a = b = 0.0;
     if (j > e1) return;
-    if (j >= seg_lo[0]) {
-      a = section_score(S, r0, q, j);
+    int ch = -1;
+    if (n <= kChain) {
+      for (int g = 0; g < n; ++g)
+        if (ch < 0 && j >= seg_lo[g]) ch = seg_ch[g];
     } else {
-      int ch = -1;
-      if (n <= kChain) {
-        for (int g = 1; g < n; ++g)
-          if (ch < 0 && j >= seg_lo[g]) ch = seg_ch[g];
-      } else {
-        int x = prev[i];
-        while (x != 0 && j < from[x]) x = prev[x];
-        ch = pch[x];
-      }
-      a = section_score(S, section_row(S, ch), q, j);
+      int x = prev[i];
+      while (x != 0 && j < from[x]) x = prev[x];
+      ch = pch[x];
     }
+    a = section_score(S, section_row(S, ch), q, j);
     b = section_score(S, ri, q, j);
   });
 }
