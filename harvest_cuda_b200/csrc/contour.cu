@@ -835,35 +835,34 @@ __global__ void __launch_bounds__(kContourThreads, 2) contour_extend(ContourView
 // fetch(j).b, each added in frame order as the reference does; fetch returns
 // 0, 0 for j > hi. Scores are nonnegative, so each ordered sum lies within
 // (n - 1) u relative of the exact one, as does the warp's sum in any order:
-// the lanes take 32 frames at a time (the next 32 fetched first) and reduce
-// them by a tree. The decision is taken from those sums when they differ by
-// more than both errors can explain; when the two sides hold the same score
-// at every frame the reference's sums are equal (not larger); otherwise (or
-// if a sum is not finite) the warp repeats the ordered sums exactly.
+// each lane adds its frames (up to 8 rounds of 32 fetched at once) and the
+// lanes' sums are reduced by one tree. The decision is taken from those
+// sums when they differ by more than both errors can explain; when the two
+// sides hold the same score at every frame the reference's sums are equal
+// (not larger); otherwise (or if a sum is not finite) the warp repeats the
+// ordered sums exactly.
 template <class Fetch>
 __device__ bool merge_sum_larger(int lo, int hi, Fetch fetch) {
   constexpr int kRounds = 8;   // rounds of 32 frames loaded before any is added
   const int lane = threadIdx.x & 31;
-  double t1 = 0.0, t2 = 0.0;
-  bool differ = false;
+  double t1 = 0.0, t2 = 0.0;   // this lane's partial sums, reduced once at the end
+  bool mine = false;
   for (int c0 = lo; c0 <= hi; c0 += 32 * kRounds) {
     double a[kRounds], b[kRounds];
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) fetch(c0 + 32 * r + lane, a[r], b[r]);
 #pragma unroll
     for (int r = 0; r < kRounds; ++r) {
-      if (c0 + 32 * r > hi) break;
-      differ |= __any_sync(kAll, a[r] != b[r]);
-      double ra = a[r], rb = b[r];
-      for (int o = 16; o; o >>= 1) {
-        ra += __shfl_xor_sync(kAll, ra, o);
-        rb += __shfl_xor_sync(kAll, rb, o);
-      }
-      t1 += ra;
-      t2 += rb;
+      mine |= a[r] != b[r];
+      t1 += a[r];
+      t2 += b[r];
     }
   }
-  if (!differ) return false;
+  for (int o = 16; o; o >>= 1) {
+    t1 += __shfl_xor_sync(kAll, t1, o);
+    t2 += __shfl_xor_sync(kAll, t2, o);
+  }
+  if (!__any_sync(kAll, mine)) return false;
   const double n = hi - lo + 1;
   constexpr double u = 1.1102230246251565e-16;   // 2^-53
   if (fabs(t1 - t2) > 4.0 * (n + 2.0) * u * (t1 + t2) && t1 + t2 <= 1.0e300) return t1 > t2;
