@@ -1536,6 +1536,96 @@ __global__ void record_tape(ContourView v, const double* __restrict__ cand, int6
   tape[2 * gf + 1] = f0c;
 }
 
+// Sections at least this long have their smoothing adjoint run by the whole
+// warp; shorter ones run one per lane.
+constexpr int kAdjointLong = 1024;
+// Steps a lane of adjoint_section_warp runs from a zero state before its
+// chunk: the skipped state's influence falls below 0.875^256 (1.5e-15) of it.
+constexpr int kAdjointWarm = 256;
+
+// The smoothing adjoint of one long section [st, ed] by the whole warp. The
+// forward pass runs over [st, ed + trailing] (the section's gradient, then
+// zeros), its outputs past ed going to `tail` (kAdjointTail doubles); the
+// backward pass runs over [st - leading, ed + trailing] on the forward
+// outputs (zero before st), its outputs past either end summed into the end
+// frames. Each pass is cut into 32 chunks, one per lane; a lane starts
+// kAdjointWarm steps before its chunk from a zero state, or from the pass's
+// own zero start where that is reached, so the result equals the one-lane
+// loop of contour_adjoint up to rounding and terms below 0.875^kAdjointWarm.
+__device__ void adjoint_section_warp(const double* __restrict__ g_sm, double* __restrict__ body,
+                                     double* __restrict__ g_s4, double* __restrict__ tail, int st, int ed,
+                                     int leading, int trailing) {
+  const int lag = 300, lane = threadIdx.x & 31;
+  constexpr int kAhead = 2 * kChunk;   // inputs loaded ahead into registers
+  const int e = ed + trailing;
+  {
+    const int n = e - st + 1, chunk = (n + 31) / 32;
+    const int c0 = imin(st + lane * chunk, e + 1), c1 = imin(c0 + chunk, e + 1);   // this lane's [c0, c1)
+    Butter fw;
+    auto run = [&](int from, int to, bool store) {   // steps from .. to - 1
+      for (int j0 = from; j0 < to; j0 += kAhead) {
+        double in[kAhead];
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) in[k] = j0 + k < to && j0 + k <= ed ? g_sm[j0 + k - lag] : 0.0;
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) {
+          const int j = j0 + k;
+          if (j >= to) break;
+          const double o = fw.step(in[k]);
+          if (store) {
+            if (j <= ed) body[j - lag] = o;
+            else tail[j - ed - 1] = o;
+          }
+        }
+      }
+    };
+    run(imax(st, c0 - kAdjointWarm), c0, false);
+    run(c0, c1, true);
+  }
+  __syncwarp();
+  const int s = st - leading;
+  double held_st = 0.0, held_ed = 0.0;
+  {
+    const int n = e - s + 1, chunk = (n + 31) / 32;
+    const int c0 = imin(s + lane * chunk, e + 1), c1 = imin(c0 + chunk, e + 1);
+    Butter bw;
+    auto run = [&](int from, int to, bool store) {   // steps from down to to
+      for (int j0 = from; j0 >= to; j0 -= kAhead) {
+        double in[kAhead];
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) {
+          const int j = j0 - k;
+          in[k] = j < to || j < st ? 0.0 : j <= ed ? body[j - lag] : tail[j - ed - 1];
+        }
+#pragma unroll
+        for (int k = 0; k < kAhead; ++k) {
+          const int j = j0 - k;
+          if (j < to) break;
+          const double o = bw.step(in[k]);
+          if (store) {
+            if (j > ed) held_ed += o;
+            else if (j >= st) g_s4[j - lag] = o;
+            else held_st += o;
+          }
+        }
+      }
+    };
+    run(imin(e, c1 - 1 + kAdjointWarm), c1, false);
+    run(c1 - 1, c0, true);
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    held_st += __shfl_xor_sync(kAll, held_st, o);
+    held_ed += __shfl_xor_sync(kAll, held_ed, o);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    g_s4[ed - lag] += held_ed;
+    g_s4[st - lag] += held_st;
+  }
+  __syncwarp();
+}
+
 // Transpose of the resampling, SmoothF0Contour and FixStep4 for the F0
 // gradient, with the voicing held fixed; one warp per clip. From dL/df0 at
 // the output frames it forms dL/d(step-3 value) per 1 ms frame:
@@ -1592,27 +1682,66 @@ __global__ void __launch_bounds__(32) contour_adjoint(GradView v) {
     }
   }
   __syncwarp();
-  // Smoothing, one voiced section of the padded contour per lane.
+  // Smoothing: each voiced section of the padded contour shorter than
+  // kAdjointLong on one lane, the longer ones by the whole warp after them.
+  // The lanes' free responses past their sections' ends sit interleaved in
+  // `tails` (step k of lane l at k * 32 + l), so their stores and loads
+  // coalesce; the sequential loops load kAhead inputs ahead into registers.
   const int lag = 300;
-  const int64_t len = F + 2 * lag;
+  const int len = F + 2 * lag;
+  constexpr int kAhead = 2 * kChunk;
   auto padded = [&](int j) -> double { return (j >= lag && j < lag + F) ? s4[j - lag] : 0.0; };
-  const int nbs = warp_boundary_list(padded, static_cast<int>(len), bl);
+  const int nbs = warp_boundary_list(padded, len, bl);
   for (int sec = lane; sec < nbs / 2; sec += 32) {
     const int st = bl[2 * sec], ed = bl[2 * sec + 1];
+    if (ed - st + 1 >= kAdjointLong) continue;
     Butter fw;
-    for (int j = st; j <= ed; ++j) body[j - lag] = fw.step(g_sm[j - lag]);
-    double* tail = tails + lane * kTransient;
-    const int64_t trailing = len - 1 - ed < kAdjointTail ? len - 1 - ed : kAdjointTail;
-    for (int64_t k = 0; k < trailing; ++k) tail[k] = fw.step(0.0);
+    for (int j0 = st; j0 <= ed; j0 += kAhead) {
+      double in[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) in[k] = j0 + k <= ed ? g_sm[j0 + k - lag] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) {
+        if (j0 + k > ed) break;
+        body[j0 + k - lag] = fw.step(in[k]);
+      }
+    }
+    const int trailing = imin(len - 1 - ed, kAdjointTail);
+    for (int k = 0; k < trailing; ++k) tails[k * 32 + lane] = fw.step(0.0);
     Butter bw;
     double held = 0.0;
-    for (int64_t k = trailing - 1; k >= 0; --k) held += bw.step(tail[k]);
-    for (int j = ed; j >= st; --j) g_s4[j - lag] = bw.step(body[j - lag]);
+    for (int k0 = trailing - 1; k0 >= 0; k0 -= kAhead) {
+      double in[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) in[k] = k0 - k >= 0 ? tails[(k0 - k) * 32 + lane] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) {
+        if (k0 - k < 0) break;
+        held += bw.step(in[k]);
+      }
+    }
+    for (int j0 = ed; j0 >= st; j0 -= kAhead) {
+      double in[kAhead];
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) in[k] = j0 - k >= st ? body[j0 - k - lag] : 0.0;
+#pragma unroll
+      for (int k = 0; k < kAhead; ++k) {
+        if (j0 - k < st) break;
+        g_s4[j0 - k - lag] = bw.step(in[k]);
+      }
+    }
     g_s4[ed - lag] += held;
     held = 0.0;
-    const int leading = st < kAdjointTail ? st : kAdjointTail;
+    const int leading = imin(st, kAdjointTail);
     for (int k = 0; k < leading; ++k) held += bw.step(0.0);
     g_s4[st - lag] += held;
+  }
+  __syncwarp();
+  for (int sec = 0; sec < nbs / 2; ++sec) {
+    const int st = bl[2 * sec], ed = bl[2 * sec + 1];
+    if (ed - st + 1 < kAdjointLong) continue;
+    adjoint_section_warp(g_sm, body, g_s4, tails, st, ed, imin(st, kAdjointTail),
+                         imin(len - 1 - ed, kAdjointTail));
   }
   __syncwarp();
   // FixStep4: unfilled frames pass through; each gap then adds to its left
