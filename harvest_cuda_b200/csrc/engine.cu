@@ -267,6 +267,7 @@ struct Workspace {
   cudaStream_t stream = nullptr;
   cudaEvent_t marks[HV_STAGE_COUNT + 1] = {};
   cudaEvent_t last = nullptr;  // completion of the previous call's work
+  cudaEvent_t fork = nullptr, join = nullptr;   // the backward pass's side branch on `stream`
   GrowingBuffer arena;          // the plans' device arena
   int sms = 0;
   double2* twiddles = nullptr;  // e^{-2 pi i t / 8192}, t < 8192
@@ -292,6 +293,8 @@ struct Workspace {
     check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "cudaStreamCreate");
     for (auto& e : marks) check(cudaEventCreate(&e), "cudaEventCreate");
     check(cudaEventCreateWithFlags(&last, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&join, cudaEventDisableTiming), "cudaEventCreate");
     check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
     check(cudaMalloc(&twiddles, sizeof(double2) * fft_bank_block_length()), "cudaMalloc(twiddles)");
     check(cudaHostAlloc(reinterpret_cast<void**>(&host_flag), sizeof(int), cudaHostAllocDefault), "cudaHostAlloc");
@@ -313,6 +316,8 @@ struct Workspace {
       if (host_flag) cudaFreeHost(host_flag);
       for (auto& e : marks) if (e) cudaEventDestroy(e);
       if (last) cudaEventDestroy(last);
+      if (fork) cudaEventDestroy(fork);
+      if (join) cudaEventDestroy(join);
       if (stream) cudaStreamDestroy(stream);
     } catch (...) {
     }
@@ -761,13 +766,14 @@ struct Workspace {
 
   // Backward pass of the F0 gradient: dL/dx for the clips at `x` from dL/df0
   // and the forward pass's tape. The waveform y is recomputed from x; the
-  // adjoints run in reverse stage order.
+  // adjoints run in reverse stage order. The contour's adjoint reads only the
+  // tape and dL/df0, so it runs on the workspace's stream, forked from and
+  // joined back into `s`, while `s` recomputes the waveform.
   void enqueue_backward(Plan& p, const double* x, const double* tape, const double* grad_f0, double* grad_x,
                         cudaStream_t s) {
     const int B = p.clips;
     const int64_t F = p.frame_off[B];
     const BatchView bv = batch_view(p);
-    enqueue_waveform(p, x, s);
     GradView gv{};
     gv.batch = bv;
     gv.tape = tape;
@@ -775,9 +781,14 @@ struct Workspace {
     gv.period = p.s.period; gv.out_off = p.d_out_off;
     gv.grad_f0 = grad_f0;
     gv.grad_fixed = ptr<double>(p.at.grad_fixed);
-    check(launch_contour_adjoint(gv, s), "contour_adjoint");
+    check(cudaEventRecord(fork, s), "cudaEventRecord");
+    check(cudaStreamWaitEvent(stream, fork, 0), "cudaStreamWaitEvent");
+    check(launch_contour_adjoint(gv, stream), "contour_adjoint");
+    check(cudaEventRecord(join, stream), "cudaEventRecord");
+    enqueue_waveform(p, x, s);
     double* grad_y = ptr<double>(p.at.grad_y);
     check(cudaMemsetAsync(grad_y, 0, 8 * p.y_off[B], s), "memset");
+    check(cudaStreamWaitEvent(s, join, 0), "cudaStreamWaitEvent");
     check(launch_refine_adjoint(bv, ptr<double>(p.at.y), tape, gv.grad_fixed, F, twiddles, grad_y, sms, s),
           "refine_adjoint");
     check(launch_remove_mean_adjoint(bv, grad_y, s), "remove_mean_adjoint");
