@@ -69,7 +69,9 @@ def test_tape_matches_checker(gpu, checker):
     assert np.all(tape[tape[:, 0] > 0, 1] > 0)
 
 
-@pytest.mark.parametrize("fs,seconds", [(16000, 0.9), (44100, 0.6)])
+# The longer clips hold voiced sections of more than 1024 frames, whose
+# smoothing adjoint the whole warp runs in chunks.
+@pytest.mark.parametrize("fs,seconds", [(16000, 0.9), (44100, 0.6), (16000, 1.8), (44100, 1.4)])
 def test_gradient_matches_torch_reference(gpu, fs, seconds):
     torch = _torch()
     made = [signals.glide_clip(seconds, fs, edge=0.15, seed=s) for s in (11, 12)]
