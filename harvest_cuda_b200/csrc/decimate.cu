@@ -226,27 +226,55 @@ __global__ void adjoint_edges(DecimateView v, const double* __restrict__ states,
   if (n > 1) gx[v.x_off[c] + n - 1] = last;
 }
 
-// Transpose of the DC removal: g -= mean(g) per clip, with the same fixed
-// reduction tree as remove_mean_and_edge_bins.
-__global__ void remove_mean_adjoint(const BatchView v, double* __restrict__ g) {
-  __shared__ double part[32];
-  int c = blockIdx.x;
-  int64_t begin = v.y_off[c], len = v.y_off[c + 1] - begin;
-  double* gc = g + begin;
-  double acc = 0.0;
-  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) acc += gc[i];
-  for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  if (!lane) part[warp] = acc;
+constexpr int kDcThreads = 256;
+
+// Sum over the block of each thread's kN values, in a fixed tree (warp
+// shuffles, then the warps' sums by warp 0); the sums are valid in thread 0.
+template <int kN>
+__device__ __forceinline__ void block_sum(double (&v)[kN], double (*part)[kDcThreads / 32]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < kN; ++j)
+    for (int o = 16; o; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+  if (lane == 0)
+#pragma unroll
+    for (int j = 0; j < kN; ++j) part[j][warp] = v[j];
   __syncthreads();
   if (warp == 0) {
-    acc = lane < warps ? part[lane] : 0.0;
-    for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (!lane) part[0] = acc;
+#pragma unroll
+    for (int j = 0; j < kN; ++j) {
+      v[j] = lane < kDcThreads / 32 ? part[j][lane] : 0.0;
+      for (int o = 16; o; o >>= 1) v[j] += __shfl_down_sync(0xffffffffu, v[j], o);
+    }
+  }
+}
+
+// Word w of clip c's chunk parts added over its chunks by one full warp
+// (lane l takes chunks l, l + 32, ... in order, then a shuffle tree); every
+// lane returns the sum, the same in every block that asks.
+__device__ __forceinline__ double clip_chunk_sum(const DcChunks& d, int c, int w) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int64_t j = d.chunk_off[c] + lane; j < d.chunk_off[c + 1]; j += 32) s += d.parts[4 * j + w];
+  for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  return s;
+}
+
+// Transpose of the DC removal: g -= mean(g) per clip, the mean formed from
+// dc_chunk_sums' chunk sums as dc_remove forms it.
+__global__ void __launch_bounds__(kDcThreads) dc_subtract(const BatchView v, DcChunks d, double* __restrict__ g) {
+  __shared__ double s_mean;
+  const int64_t k = blockIdx.x;
+  const int c = owner(d.chunk_off, v.clips, k);
+  const int64_t begin = v.y_off[c], len = v.y_off[c + 1] - begin;
+  if (threadIdx.x < 32) {
+    const double sum = clip_chunk_sum(d, c, 0);
+    if (threadIdx.x == 0) s_mean = sum / len;
   }
   __syncthreads();
-  const double mean = part[0] / len;
-  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) gc[i] -= mean;
+  const double mean = s_mean;
+  const int64_t lo = (k - d.chunk_off[c]) * kDcChunk, hi = lo + kDcChunk < len ? lo + kDcChunk : len;
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kDcThreads) g[begin + i] -= mean;
 }
 
 // Sets *flag if any sample is not finite (the reference rejects such input,
@@ -272,62 +300,73 @@ __global__ void copy_clips(const double* __restrict__ x, int64_t total, double* 
   if (i < total) y[i] = x[i];
 }
 
-// a3 (harvest.cpp:82-86): y -= mean(y), one block per clip with a fixed
-// reduction tree (deterministic). Also returns the two spectrum bins that
+// a3 (harvest.cpp:82-86): y -= mean(y). Also the two spectrum bins that
 // WORLD's band filter overwrites (harvest.cpp:116-133): Y[n/2] and Y[n/2-1]
-// of the zero-padded n-point transform, for the final-bin correction.
-__global__ void remove_mean_and_edge_bins(const BatchView v, double* __restrict__ y,
-                                          double* __restrict__ bins /* 3 per clip */) {
-  __shared__ double part[3][32];
-  int c = blockIdx.x;
-  int64_t begin = v.y_off[c], len = v.y_off[c + 1] - begin;
-  double* yc = y + begin;
-  double acc = 0.0;
-  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) acc += yc[i];
-  // Block reduction of the sum.
-  for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
-  if (!lane) part[0][warp] = acc;
-  __syncthreads();
-  if (warp == 0) {
-    acc = lane < warps ? part[0][lane] : 0.0;
-    for (int o = 16; o; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
-    if (!lane) part[0][0] = acc;
+// of the zero-padded n-point transform, for the final-bin correction. Each
+// clip is cut into chunks of kDcChunk samples, a block per chunk, so that a
+// long clip spreads over many SMs; every sum has a fixed order (a tree
+// within a chunk, then the clip's chunks by lane and a shuffle tree), so a
+// clip's results do not depend on the batch around it:
+//   dc_chunk_sums: parts[4 k] = the sum of chunk k's samples;
+//   dc_remove:     each block forms its clip's mean from the chunk sums (the
+//                  same additions in every block), subtracts it and writes
+//                  its chunk's three bin sums to parts[4 k + 1 .. 3];
+//   dc_edge_bins:  a warp per clip adds its chunks' bin sums.
+__global__ void __launch_bounds__(kDcThreads) dc_chunk_sums(const BatchView v, DcChunks d,
+                                                             const double* __restrict__ y) {
+  __shared__ double part[1][kDcThreads / 32];
+  const int64_t k = blockIdx.x;
+  const int c = owner(d.chunk_off, v.clips, k);
+  const int64_t begin = v.y_off[c], len = v.y_off[c + 1] - begin;
+  const int64_t lo = (k - d.chunk_off[c]) * kDcChunk, hi = lo + kDcChunk < len ? lo + kDcChunk : len;
+  double acc[1] = {0.0};
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kDcThreads) acc[0] += y[begin + i];
+  block_sum(acc, part);
+  if (threadIdx.x == 0) d.parts[4 * k] = acc[0];
+}
+
+__global__ void __launch_bounds__(kDcThreads) dc_remove(const BatchView v, DcChunks d, double* __restrict__ y) {
+  __shared__ double part[3][kDcThreads / 32];
+  __shared__ double s_mean;
+  const int64_t k = blockIdx.x;
+  const int c = owner(d.chunk_off, v.clips, k);
+  const int64_t begin = v.y_off[c], len = v.y_off[c + 1] - begin;
+  if (threadIdx.x < 32) {
+    const double sum = clip_chunk_sum(d, c, 0);
+    if (threadIdx.x == 0) s_mean = sum / len;
   }
   __syncthreads();
-  double mean = part[0][0] / len;
-  __syncthreads();
-  // Subtract, and accumulate Y[n/2] = sum y_j (-1)^j and
-  // Y[n/2-1] = sum y_j (-1)^j e^{+2 pi i j / n}.
+  const double mean = s_mean;
   const int n = v.nfft[c];
-  double ny = 0.0, br = 0.0, bi = 0.0;
-  for (int64_t i = threadIdx.x; i < len; i += blockDim.x) {
-    double val = yc[i] - mean;
-    yc[i] = val;
-    double sg = (i & 1) ? -val : val;
-    ny += sg;
-    double s, co;
-    sincospi(2.0 * static_cast<double>(i) / n, &s, &co);
-    br += sg * co;
-    bi += sg * s;
+  const int64_t lo = (k - d.chunk_off[c]) * kDcChunk, hi = lo + kDcChunk < len ? lo + kDcChunk : len;
+  // Y[n/2] = sum y_j (-1)^j and Y[n/2-1] = sum y_j (-1)^j e^{+2 pi i j / n}.
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (int64_t i = lo + threadIdx.x; i < hi; i += kDcThreads) {
+    const double val = y[begin + i] - mean;
+    y[begin + i] = val;
+    const double sg = (i & 1) ? -val : val;
+    acc[0] += sg;
+    double sn, cs;
+    sincospi(2.0 * static_cast<double>(i) / n, &sn, &cs);
+    acc[1] += sg * cs;
+    acc[2] += sg * sn;
   }
-  for (int o = 16; o; o >>= 1) {
-    ny += __shfl_down_sync(0xffffffffu, ny, o);
-    br += __shfl_down_sync(0xffffffffu, br, o);
-    bi += __shfl_down_sync(0xffffffffu, bi, o);
+  block_sum(acc, part);
+  if (threadIdx.x == 0) {
+    d.parts[4 * k + 1] = acc[0];
+    d.parts[4 * k + 2] = acc[1];
+    d.parts[4 * k + 3] = acc[2];
   }
-  if (!lane) { part[0][warp] = ny; part[1][warp] = br; part[2][warp] = bi; }
-  __syncthreads();
-  if (warp == 0) {
-    ny = lane < warps ? part[0][lane] : 0.0;
-    br = lane < warps ? part[1][lane] : 0.0;
-    bi = lane < warps ? part[2][lane] : 0.0;
-    for (int o = 16; o; o >>= 1) {
-      ny += __shfl_down_sync(0xffffffffu, ny, o);
-      br += __shfl_down_sync(0xffffffffu, br, o);
-      bi += __shfl_down_sync(0xffffffffu, bi, o);
-    }
-    if (!lane) { bins[3 * c] = ny; bins[3 * c + 1] = br; bins[3 * c + 2] = bi; }
+}
+
+__global__ void dc_edge_bins(const BatchView v, DcChunks d, double* __restrict__ bins /* 3 per clip */) {
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= v.clips) return;   // uniform per warp
+  const double ny = clip_chunk_sum(d, c, 1), br = clip_chunk_sum(d, c, 2), bi = clip_chunk_sum(d, c, 3);
+  if ((threadIdx.x & 31) == 0) {
+    bins[3 * c] = ny;
+    bins[3 * c + 1] = br;
+    bins[3 * c + 2] = bi;
   }
 }
 
@@ -404,7 +443,9 @@ cudaError_t preload_decimation_kernels() {
   load(reinterpret_cast<const void*>(decimate_forward_staged));
   load(reinterpret_cast<const void*>(decimate_segment_run<1>));
   load(reinterpret_cast<const void*>(copy_clips));
-  load(reinterpret_cast<const void*>(remove_mean_and_edge_bins));
+  load(reinterpret_cast<const void*>(dc_chunk_sums));
+  load(reinterpret_cast<const void*>(dc_remove));
+  load(reinterpret_cast<const void*>(dc_edge_bins));
   return e;
 }
 
@@ -419,13 +460,18 @@ cudaError_t launch_copy(const double* x, int64_t total, double* y, cudaStream_t 
   return cudaGetLastError();
 }
 
-cudaError_t launch_remove_mean(const BatchView& v, double* y, double* bins, cudaStream_t stream) {
-  remove_mean_and_edge_bins<<<v.clips, 1024, 0, stream>>>(v, y, bins);
+cudaError_t launch_remove_mean(const BatchView& v, const DcChunks& d, double* y, double* bins, cudaStream_t stream) {
+  const unsigned chunks = static_cast<unsigned>(d.total);
+  dc_chunk_sums<<<chunks, kDcThreads, 0, stream>>>(v, d, y);
+  dc_remove<<<chunks, kDcThreads, 0, stream>>>(v, d, y);
+  dc_edge_bins<<<(v.clips + 7) / 8, 256, 0, stream>>>(v, d, bins);
   return cudaGetLastError();
 }
 
-cudaError_t launch_remove_mean_adjoint(const BatchView& v, double* grad_y, cudaStream_t stream) {
-  remove_mean_adjoint<<<v.clips, 1024, 0, stream>>>(v, grad_y);
+cudaError_t launch_remove_mean_adjoint(const BatchView& v, const DcChunks& d, double* grad_y, cudaStream_t stream) {
+  const unsigned chunks = static_cast<unsigned>(d.total);
+  dc_chunk_sums<<<chunks, kDcThreads, 0, stream>>>(v, d, grad_y);
+  dc_subtract<<<chunks, kDcThreads, 0, stream>>>(v, d, grad_y);
   return cudaGetLastError();
 }
 

@@ -182,6 +182,7 @@ struct Plan {
   std::shared_ptr<const BankTables> bank;
   // Host copies of the per-clip tables.
   std::vector<int64_t> x_off, y_off, t_off, seg_off, frame_off, out_off, scratch_off;
+  std::vector<int64_t> dc_off;   // the DC removal's chunks per clip (kDcChunk samples of y each)
   std::vector<int> nfft;
   std::vector<int2> items;
   int64_t slot_capacity = 0, total_seg = 0;
@@ -195,11 +196,12 @@ struct Plan {
   // head of the arena by Workspace::prepare when another plan used it last.
   uint64_t id = 0;
   std::vector<char> meta;
-  size_t o_x = 0, o_y = 0, o_t = 0, o_s = 0, o_f = 0, o_o = 0, o_sc = 0, o_n = 0, o_it = 0, o_bo = 0;
+  size_t o_x = 0, o_y = 0, o_t = 0, o_s = 0, o_f = 0, o_o = 0, o_sc = 0, o_n = 0, o_it = 0, o_bo = 0, o_dc = 0;
   size_t arena_bytes = 0;
   struct Layout {
     size_t meta, pcm, x, u, states, y, bins, queue, flag, slots, spectra, raw, cand, count, jobs, classes, refined, scores,
-        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed, keys, leaders, item_off;
+        pruned, pruned_scores, best, smoothed, scratch, f0, times, grad_y, grad_fixed, keys, leaders, item_off,
+        dc_parts;
   } at{};
   int bank_ctas = 0;
   // Device pointers, set by Workspace::prepare: into the arena's copy of
@@ -210,6 +212,7 @@ struct Plan {
   double *d_centre, *d_taps;
   int2* d_items;
   int64_t* d_blk_off = nullptr;
+  int64_t* d_dc_off = nullptr;
   double* filters = nullptr;   // [bands][4097] filter amplitudes of the FFT bank
   // Refinement launch shape and contour extension blocks per clip, chosen by
   // the autotuner on the plan's first run (extend_blocks 0: the default).
@@ -404,6 +407,7 @@ struct Workspace {
     p.d_nfft = reinterpret_cast<int*>(m + p.o_n);
     p.d_items = reinterpret_cast<int2*>(m + p.o_it);
     p.d_blk_off = reinterpret_cast<int64_t*>(m + p.o_bo);
+    p.d_dc_off = reinterpret_cast<int64_t*>(m + p.o_dc);
     DeviceBank& b = device_bank(s, *p.bank, p.use_fft);
     p.d_centre = b.centre;
     p.d_half = b.half;
@@ -459,6 +463,7 @@ struct Workspace {
     p->x_off.assign(B + 1, 0); p->y_off.assign(B + 1, 0); p->t_off.assign(B + 1, 0);
     p->seg_off.assign(B + 1, 0); p->frame_off.assign(B + 1, 0); p->out_off.assign(B + 1, 0);
     p->scratch_off.assign(B + 1, 0);
+    p->dc_off.assign(B + 1, 0);
     p->nfft.assign(B, 0);
     for (int c = 0; c < B; ++c) {
       int64_t n = p->lengths[c];
@@ -467,6 +472,7 @@ struct Workspace {
       int frames = samples_for(s.fs, n, 1.0);
       p->x_off[c + 1] = p->x_off[c] + n;
       p->y_off[c + 1] = p->y_off[c] + y_len;
+      p->dc_off[c + 1] = p->dc_off[c] + dc_chunk_count(y_len);
       p->t_off[c + 1] = p->t_off[c] + (p->ratio > 1 ? total : 0);
       p->seg_off[c + 1] = p->seg_off[c] + (p->ratio > 1 ? (total + kSegment - 1) / kSegment : 0);
       p->frame_off[c + 1] = p->frame_off[c] + frames;
@@ -536,6 +542,7 @@ struct Workspace {
     p->o_n = put(p->nfft.data(), 4 * B);
     p->o_it = put(p->items.data(), sizeof(int2) * p->items.size());
     p->o_bo = put(p->blk_off.data(), 8 * (B + 1));
+    p->o_dc = put(p->dc_off.data(), 8 * (B + 1));
     if (p->use_fft && fft_bank_ctas_per_sm() < 1)
       throw RuntimeFailure("FFT band-bank kernel does not fit on this device");
     // Arena layout.
@@ -555,6 +562,7 @@ struct Workspace {
     p->at.states = take(8 * 6 * p->total_seg);   // zero-state results, chained initial states
     p->at.y = take(8 * p->y_off[B]);
     p->at.bins = take(8 * 3 * B);
+    p->at.dc_parts = take(8 * 4 * p->dc_off[B]);
     p->at.queue = take(16);
     p->at.flag = take(16);
     p->at.slots = take(8 * 4 * p->slot_capacity * p->bank_ctas);
@@ -584,6 +592,10 @@ struct Workspace {
 
   template <class T>
   T* ptr(size_t at) const { return reinterpret_cast<T*>(static_cast<char*>(arena.ptr) + at); }
+
+  DcChunks dc_view(const Plan& p) const {
+    return DcChunks{p.d_dc_off, p.dc_off[p.clips], ptr<double>(p.at.dc_parts)};
+  }
 
   static BatchView batch_view(const Plan& p) {
     BatchView bv{};
@@ -646,7 +658,7 @@ struct Workspace {
             "decimate");
     else
       check(launch_copy(x, p.x_off[p.clips], y, s), "copy");
-    check(launch_remove_mean(batch_view(p), y, ptr<double>(p.at.bins), s), "remove_mean");
+    check(launch_remove_mean(batch_view(p), dc_view(p), y, ptr<double>(p.at.bins), s), "remove_mean");
   }
 
   // Enqueues every stage on `s`. With `marks_on`, records stage events.
@@ -755,7 +767,7 @@ struct Workspace {
     double* grad_y = ptr<double>(p.at.grad_y);
     check(launch_band_correlate(rv.batch, grad_f, y_total, p.d_half, p.d_tap_off, p.d_taps, grad_y, s),
           "band_correlate");
-    check(launch_remove_mean_adjoint(rv.batch, grad_y, s), "remove_mean_adjoint");
+    check(launch_remove_mean_adjoint(rv.batch, dc_view(p), grad_y, s), "remove_mean_adjoint");
     if (p.ratio > 1)
       check(launch_decimate_adjoint(decimate_view(p), grad_y, ptr<double>(p.at.u), ptr<double>(p.at.states),
                                     p.total_seg, grad_x, s),
@@ -791,7 +803,7 @@ struct Workspace {
     check(cudaStreamWaitEvent(s, join, 0), "cudaStreamWaitEvent");
     check(launch_refine_adjoint(bv, ptr<double>(p.at.y), tape, gv.grad_fixed, F, twiddles, grad_y, sms, s),
           "refine_adjoint");
-    check(launch_remove_mean_adjoint(bv, grad_y, s), "remove_mean_adjoint");
+    check(launch_remove_mean_adjoint(bv, dc_view(p), grad_y, s), "remove_mean_adjoint");
     if (p.ratio > 1)
       check(launch_decimate_adjoint(decimate_view(p), grad_y, ptr<double>(p.at.u), ptr<double>(p.at.states),
                                     p.total_seg, grad_x, s),
@@ -1004,9 +1016,10 @@ void validate_batch(const int64_t* offsets, int clips, int fs, double f0_floor, 
 // Scratch of hv_decimate_noalloc: a fixed array in the library's device
 // image, present on every GPU that loads the library for the life of the
 // process. It holds the forward low-pass pass (n + 2 lag + 18 doubles), the
-// segment states (6 per 256 samples) and a 16-word tail: the offset tables
-// (words 0-7), the FFT size (word 8) and the three edge bins (words 10-12)
-// that the DC-removal kernel writes.
+// segment states (6 per 256 samples), a 16-word tail: the offset tables
+// (words 0-7), the FFT size (word 8), the three edge bins (words 10-12)
+// that the DC removal writes and its chunk table (words 14-15), and the DC
+// removal's 4 doubles per chunk.
 constexpr int max_decimation_lag() {
   int m = 0;
   for (int r = 2; r <= 12; ++r) m = decimation_lag(r) > m ? decimation_lag(r) : m;
@@ -1018,17 +1031,19 @@ constexpr int64_t kNoAllocMaxSamples = int64_t(1) << 20;
 constexpr int64_t kNoAllocPadded = kNoAllocMaxSamples + 2 * kNoAllocMaxLag + 18;
 constexpr int64_t kNoAllocSegments = (kNoAllocPadded + kSegment - 1) / kSegment;
 constexpr int64_t kNoAllocMeta = 16;
-constexpr int64_t kNoAllocDoubles = kNoAllocPadded + 6 * kNoAllocSegments + kNoAllocMeta;
+constexpr int64_t kNoAllocDcChunks = (kNoAllocMaxSamples + kDcChunk - 1) / kDcChunk;   // y has at most n samples
+constexpr int64_t kNoAllocDoubles = kNoAllocPadded + 6 * kNoAllocSegments + kNoAllocMeta + 4 * kNoAllocDcChunks;
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
 // Writes the one-clip offset tables into the scratch (no host copies).
 __global__ void noalloc_tables(int64_t* meta, int64_t n, int64_t y_len, int64_t padded, int64_t segments,
-                               int nfft) {
+                               int nfft, int64_t dc_chunks) {
   meta[0] = 0; meta[1] = n;          // x_off
   meta[2] = 0; meta[3] = y_len;      // y_off
   meta[4] = 0; meta[5] = padded;     // t_off
   meta[6] = 0; meta[7] = segments;   // seg_off
   reinterpret_cast<int*>(meta + 8)[0] = nfft;
+  meta[14] = 0; meta[15] = dc_chunks;   // the DC removal's chunk table
 }
 
 // Per device: the retained primary context and the scratch's device address,
@@ -1410,9 +1425,10 @@ int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* 
     double* states = u + kNoAllocPadded;
     int64_t* meta = reinterpret_cast<int64_t*>(states + 6 * kNoAllocSegments);
     double* bins = reinterpret_cast<double*>(meta + 10);
-    noalloc_tables<<<1, 1, 0, s>>>(meta, n, y_len, padded, segments, static_cast<int>(2 * y_len));
+    const DcChunks dc{meta + 14, dc_chunk_count(y_len), reinterpret_cast<double*>(meta + kNoAllocMeta)};
+    noalloc_tables<<<1, 1, 0, s>>>(meta, n, y_len, padded, segments, static_cast<int>(2 * y_len), dc.total);
     check(cudaGetLastError(), "noalloc_tables");
-    // The DC removal reads only y_off and nfft of its batch view.
+    // The DC removal reads only clips, y_off and nfft of its batch view.
     BatchView bv{};
     bv.clips = 1; bv.ratio = ratio; bv.fs_r = double(fs) / ratio;
     bv.x_off = meta; bv.y_off = meta + 2;
@@ -1435,7 +1451,7 @@ int hv_decimate_noalloc(const double* x, int64_t n, int fs, int device, double* 
     } else {
       check(launch_copy(x, n, y, s), "copy");
     }
-    check(launch_remove_mean(bv, y, bins, s), "remove_mean");
+    check(launch_remove_mean(bv, dc, y, bins, s), "remove_mean");
   });
 }
 

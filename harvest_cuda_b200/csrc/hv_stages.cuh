@@ -102,7 +102,17 @@ cudaError_t launch_compare(const double* ref, const double* f0, const int64_t* o
                            cudaStream_t stream);
 cudaError_t launch_pcm16(const int16_t* in, int64_t total, double* out, int sms, cudaStream_t stream);
 cudaError_t launch_check_finite(const double* x, int64_t total, int* flag, int sms, cudaStream_t stream);
-cudaError_t launch_remove_mean(const BatchView& v, double* y, double* bins, cudaStream_t stream);
+// The DC removal's chunks: clip c's waveform is cut into chunks of kDcChunk
+// samples, numbered chunk_off[c] .. chunk_off[c + 1] - 1 over the batch (a
+// clip of no samples still has one), and parts holds 4 doubles per chunk.
+constexpr int kDcChunk = 8192;
+inline int64_t dc_chunk_count(int64_t samples) { return samples > 0 ? (samples + kDcChunk - 1) / kDcChunk : 1; }
+struct DcChunks {
+  const int64_t* chunk_off;   // [clips + 1]
+  int64_t total;              // chunk_off[clips]
+  double* parts;              // [total][4]
+};
+cudaError_t launch_remove_mean(const BatchView& v, const DcChunks& d, double* y, double* bins, cudaStream_t stream);
 
 size_t band_bank_smem_bytes(int max_pad_taps);
 int band_bank_tap_multiple();
@@ -201,7 +211,7 @@ cudaError_t launch_contour_adjoint(const GradView& v, cudaStream_t stream);
 cudaError_t launch_refine_adjoint(const BatchView& v, const double* y, const double* tape,
                                   const double* grad_fixed, int64_t total_frames, const double2* tw,
                                   double* grad_y, int sms, cudaStream_t stream);
-cudaError_t launch_remove_mean_adjoint(const BatchView& v, double* grad_y, cudaStream_t stream);
+cudaError_t launch_remove_mean_adjoint(const BatchView& v, const DcChunks& d, double* grad_y, cudaStream_t stream);
 cudaError_t launch_decimate_adjoint(const DecimateView& v, const double* grad_y, double* u, double* states,
                                     int64_t segments, double* grad_x, cudaStream_t stream);
 cudaError_t launch_contour(const ContourView& v, cudaStream_t stream);
