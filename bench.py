@@ -368,10 +368,11 @@ def accuracy_against(reference_f0, sample, f0, out_off, kind, device):
 
 def kernels_per_step(ratio):
     # finiteness flag; decimation (3 kernels per direction, or one copy at
-    # ratio 1); mean and edge bins; block spectra and the FFT band bank;
-    # official candidates; refinement (keys, two bucket passes, offsets,
-    # jobs); prune + best; contour (prepare, extend, finish).
-    return 1 + (6 if ratio > 1 else 1) + 1 + 2 + 1 + 5 + 1 + 3
+    # ratio 1); DC removal and edge bins (chunk sums, removal, bins); block
+    # spectra and the FFT band bank; official candidates; refinement (keys,
+    # two bucket passes, offsets, jobs); prune + best; contour (prepare,
+    # extend, finish).
+    return 1 + (6 if ratio > 1 else 1) + 3 + 2 + 1 + 5 + 1 + 3
 
 
 def fp64_peak(device):
