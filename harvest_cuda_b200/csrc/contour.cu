@@ -673,12 +673,22 @@ __device__ int extend_f0_ahead(const double* cand, const double* score, int64_t 
         const double e = fabs(cur - rc[u][q]) / cur;
         if (e <= best_e) { best_e = e; best_i = i; val = rc[u][q]; }
       }
-      for (int o = 16; o; o >>= 1) {
-        const double oe = __shfl_xor_sync(kAll, best_e, o), ov = __shfl_xor_sync(kAll, val, o);
-        const int oi = __shfl_xor_sync(kAll, best_i, o);
-        if (oi >= 0 && (best_i < 0 || oe < best_e || (oe == best_e && oi > best_i))) {
-          best_e = oe; best_i = oi; val = ov;
-        }
+      {
+        // Across the lanes: the smallest error, then the largest column. The
+        // errors map to unsigned keys in the same order (-0 taken as +0, as
+        // the comparison has them equal); the minimum key is found by its
+        // high and then its low word, the column by a maximum over the
+        // lanes holding that key, and the value from the column's lane.
+        unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(best_e + 0.0));
+        b = (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+        const unsigned long long key = best_i >= 0 ? b : ~0ull;
+        const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
+        const unsigned min_hi = __reduce_min_sync(kAll, hi);
+        const unsigned min_lo = __reduce_min_sync(kAll, hi == min_hi ? lo : ~0u);
+        const bool at_min = best_i >= 0 && hi == min_hi && lo == min_lo;
+        const unsigned top = __reduce_max_sync(kAll, at_min ? static_cast<unsigned>(best_i) + 1u : 0u);
+        const double won = __shfl_sync(kAll, val, static_cast<int>((top - 1u) & 31u));
+        val = top ? won : 0.0;
       }
       // SearchScore (harvest.cpp:901-907) of the pick in the same row.
       double sc = 0.0;
