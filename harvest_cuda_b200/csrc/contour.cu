@@ -196,6 +196,39 @@ __device__ int block_boundary_list(F f, int len, int* out, int* red) {
 // then consume them in the reference's order.
 constexpr int kChunk = 8;
 
+// Warp arg-min of SelectBestF0 over the lanes' picks (error best_e of
+// column best_i holding val; best_i < 0: none): the smallest error, the
+// later column on ties, whose value every lane returns (0 if no lane has a
+// pick). Column i sits in lane i % 32. The errors map to unsigned keys in the
+// same order (-0 as +0, which the comparison holds equal); the minimum key is
+// found by its high and then its low word, the column by a maximum over the
+// lanes holding that key: three dependent reductions and one shuffle, where
+// five rounds of shuffles and FP64 compares would chain twice as long.
+__device__ __forceinline__ double warp_pick(double best_e, int best_i, double val) {
+  unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(best_e + 0.0));
+  b = (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+  const unsigned long long key = best_i >= 0 ? b : ~0ull;
+  const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
+  const unsigned min_hi = __reduce_min_sync(kAll, hi);
+  const unsigned min_lo = __reduce_min_sync(kAll, hi == min_hi ? lo : ~0u);
+  const bool at_min = best_i >= 0 && hi == min_hi && lo == min_lo;
+  const unsigned top = __reduce_max_sync(kAll, at_min ? static_cast<unsigned>(best_i) + 1u : 0u);
+  const double won = __shfl_sync(kAll, val, static_cast<int>((top - 1u) & 31u));
+  return top ? won : 0.0;
+}
+
+// Warp maximum of SearchScore partial maxima, which are +0 or larger and
+// never NaN (a lane takes a score only when it exceeds its current maximum):
+// their bit patterns order as unsigned integers, so the maximum is found by
+// its high and then its low word.
+__device__ __forceinline__ double warp_max_score(double s) {
+  const unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(s));
+  const unsigned hi = static_cast<unsigned>(b >> 32), lo = static_cast<unsigned>(b);
+  const unsigned max_hi = __reduce_max_sync(kAll, hi);
+  const unsigned max_lo = __reduce_max_sync(kAll, hi == max_hi ? lo : 0u);
+  return __longlong_as_double(static_cast<long long>((static_cast<unsigned long long>(max_hi) << 32) | max_lo));
+}
+
 // SelectBestF0 (harvest.cpp:636-650) with the columns spread over the lanes
 // of a warp. The
 // reference's loop keeps a candidate whenever its error is at most the
@@ -212,14 +245,7 @@ __device__ __forceinline__ double warp_select_best(double ref, const double* can
     const double e = fabs(ref - c) / ref;
     if (e <= best_e) { best_e = e; best_i = i; best_v = c; }
   }
-  for (int o = 16; o; o >>= 1) {
-    const double oe = __shfl_xor_sync(kAll, best_e, o), ov = __shfl_xor_sync(kAll, best_v, o);
-    const int oi = __shfl_xor_sync(kAll, best_i, o);
-    if (oi >= 0 && (best_i < 0 || oe < best_e || (oe == best_e && oi > best_i))) {
-      best_e = oe; best_i = oi; best_v = ov;
-    }
-  }
-  return best_v;
+  return warp_pick(best_e, best_i, best_v);
 }
 
 // A candidate row held in registers, column lane + 32 k in slot k, for
@@ -249,14 +275,7 @@ __device__ __forceinline__ double warp_select_best(double ref, const CandRow& ro
     const double e = fabs(ref - c) / ref;
     if (e <= best_e) { best_e = e; best_i = i; best_v = c; }
   }
-  for (int o = 16; o; o >>= 1) {
-    const double oe = __shfl_xor_sync(kAll, best_e, o), ov = __shfl_xor_sync(kAll, best_v, o);
-    const int oi = __shfl_xor_sync(kAll, best_i, o);
-    if (oi >= 0 && (best_i < 0 || oe < best_e || (oe == best_e && oi > best_i))) {
-      best_e = oe; best_i = oi; best_v = ov;
-    }
-  }
-  return best_v;
+  return warp_pick(best_e, best_i, best_v);
 }
 
 // One direction of ExtendF0 (harvest.cpp:791-824) from frame `from` with
@@ -620,11 +639,7 @@ __device__ __forceinline__ double warp_search_score(double value, const double* 
   double s = 0.0;
   for (int i = lane; i < columns; i += 32)
     if (value == cand[i] && s < score[i]) s = score[i];
-  for (int o = 16; o; o >>= 1) {
-    const double t = __shfl_xor_sync(kAll, s, o);
-    if (s < t) s = t;
-  }
-  return s;
+  return warp_max_score(s);
 }
 
 // One direction of ExtendF0 as extend_f0, also recording the SearchScore of
@@ -673,32 +688,13 @@ __device__ int extend_f0_ahead(const double* cand, const double* score, int64_t 
         const double e = fabs(cur - rc[u][q]) / cur;
         if (e <= best_e) { best_e = e; best_i = i; val = rc[u][q]; }
       }
-      {
-        // Across the lanes: the smallest error, then the largest column. The
-        // errors map to unsigned keys in the same order (-0 taken as +0, as
-        // the comparison has them equal); the minimum key is found by its
-        // high and then its low word, the column by a maximum over the
-        // lanes holding that key, and the value from the column's lane.
-        unsigned long long b = static_cast<unsigned long long>(__double_as_longlong(best_e + 0.0));
-        b = (b >> 63) ? ~b : (b | 0x8000000000000000ull);
-        const unsigned long long key = best_i >= 0 ? b : ~0ull;
-        const unsigned hi = static_cast<unsigned>(key >> 32), lo = static_cast<unsigned>(key);
-        const unsigned min_hi = __reduce_min_sync(kAll, hi);
-        const unsigned min_lo = __reduce_min_sync(kAll, hi == min_hi ? lo : ~0u);
-        const bool at_min = best_i >= 0 && hi == min_hi && lo == min_lo;
-        const unsigned top = __reduce_max_sync(kAll, at_min ? static_cast<unsigned>(best_i) + 1u : 0u);
-        const double won = __shfl_sync(kAll, val, static_cast<int>((top - 1u) & 31u));
-        val = top ? won : 0.0;
-      }
+      val = warp_pick(best_e, best_i, val);
       // SearchScore (harvest.cpp:901-907) of the pick in the same row.
       double sc = 0.0;
 #pragma unroll
       for (int q = 0; q < NS; ++q)
         if (lane + 32 * q < columns && val == rc[u][q] && sc < rs[u][q]) sc = rs[u][q];
-      for (int o = 16; o; o >>= 1) {
-        const double t = __shfl_xor_sync(kAll, sc, o);
-        if (sc < t) sc = t;
-      }
+      sc = warp_max_score(sc);
       load(rc[u], rs[u], k + D);
       if (lane == 0) {
         out[k] = val;
@@ -764,10 +760,7 @@ __device__ void body_scores(const double* s2, const double* cand, const double* 
 #pragma unroll
       for (int q = 0; q < NS; ++q)
         if (lane + 32 * q < columns && v[f] == c[f][q] && s < sc[f][q]) s = sc[f][q];
-      for (int o = 16; o; o >>= 1) {
-        const double t = __shfl_xor_sync(kAll, s, o);
-        if (s < t) s = t;
-      }
+      s = warp_max_score(s);
       if (lane == 0 && j0 + f <= j_hi) out[j0 + f - j_lo] = s;
     }
   }
